@@ -1,0 +1,253 @@
+// GPU breadth-first search of a coset table, and the encoders of its solving files.
+//
+// What is computed is the reference's (table.py:82-129, kernels.cu:485-624,1839-1869): the exact
+// distance of every entry from the solved coset, with forward passes (expand every entry of the
+// current depth: unrank, 18 moves, claim each neighbour and its stabiliser images) while the
+// frontier is small and backward passes (an unvisited entry whose neighbour sits at the current
+// depth is one deeper) afterwards.  The files are pure functions of those distances: per 32-byte
+// sector a minimum and 2-bit offsets, or the base-3 code with a per-block cut.
+//
+// The representation is this library's own: one byte of exact depth per entry (0xFF =
+// unvisited), 30 GB for the 30.2-billion-entry tables, which B200's HBM holds next to the output.
+// A claim is a single atomicAnd on the byte's word (0xFF & (d | ~0xFF) = d; visited bytes are
+// never touched because they are tested first), backward passes write only their own bytes and
+// need no atomics, and the block / base-3 encoders are streaming passes over the depth bytes.
+#pragma once
+
+#include "cube_dev.cuh"
+
+namespace ccs {
+
+struct BfsParams {
+    uint8_t* depth;                  // n_entries bytes, padded to a multiple of 16
+    uint64_t n_entries;
+    uint64_t n_chunks;               // 16-entry chunks
+    const uint32_t* classidx;
+    const uint32_t* class_rep;
+    const uint16_t* class_stab;
+    unsigned long long* counter;     // entries found in this pass
+};
+
+__device__ __forceinline__ uint32_t claim_entry(uint8_t* depth, uint64_t idx, uint32_t d1) {
+    if (((volatile uint8_t*)depth)[idx] != 0xFFu) return 0;
+    uint32_t* w = reinterpret_cast<uint32_t*>(depth + (idx & ~3ull));
+    uint32_t sh = (uint32_t)(idx & 3u) * 8u;
+    uint32_t old = atomicAnd(w, ~(0xFFu << sh) | (d1 << sh));
+    return ((old >> sh) & 0xFFu) == 0xFFu;
+}
+
+// Claim the coset of state n and all its images under the symmetries fixing its corner class
+// representative (kernels.cu:507-528).
+template <int MODE, int NEC>
+__device__ __forceinline__ uint32_t claim_with_stabilizer(const DevTables& T, const BfsParams& P, const State& n,
+                                                          uint32_t d1) {
+    uint32_t packed = __ldg(P.classidx + corner_raw_dev(T, n));
+    uint32_t cls = packed >> 4, sym = packed & 15u;
+    uint32_t stab = __ldg(P.class_stab + cls);
+    uint64_t base = (uint64_t)cls * KindTraits<MODE, NEC>::N_EDGE;
+    uint32_t claimed = 0;
+    while (stab) {
+        uint32_t t = __ffs(stab) - 1;
+        stab &= stab - 1;
+        uint32_t e[3];
+        conj_edges(T, n, T.sym_mul[t][sym], e);
+        claimed += claim_entry(P.depth, base + edge_coord_dev<MODE, NEC>(T, e), d1);
+    }
+    return claimed;
+}
+
+__device__ __forceinline__ void add_count(unsigned long long* counter, unsigned long long local) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xFFFFFFFFu, local, o);
+    if ((threadIdx.x & 31u) == 0 && local) atomicAdd(counter, local);
+}
+
+template <int MODE, int NEC>
+__global__ void bfs_seed(const DevTables* __restrict__ gT, BfsParams P) {
+    __shared__ DevTables T;
+    stage_tables(T, gT);
+    if (threadIdx.x) return;
+    State s{0x03020100u, 0x07060504u, 0x03020100u, 0x07060504u, 0x0B0A0908u};
+    atomicAdd(P.counter, (unsigned long long)claim_with_stabilizer<MODE, NEC>(T, P, s, 0u));
+}
+
+// Forward pass: expand every entry at depth d.
+template <int MODE, int NEC>
+__global__ void __launch_bounds__(256) bfs_forward(const DevTables* __restrict__ gT, BfsParams P, uint32_t d) {
+    __shared__ DevTables T;
+    stage_tables(T, gT);
+    unsigned long long local = 0;
+    const uint4* chunks = reinterpret_cast<const uint4*>(P.depth);
+    for (uint64_t ch = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; ch < P.n_chunks;
+         ch += (uint64_t)gridDim.x * blockDim.x) {
+        uint4 v = chunks[ch];
+        uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uint32_t x = w[q] ^ (d * 0x01010101u);
+            uint32_t hit = ~(((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x | 0x7F7F7F7Fu);  // 0x80 where byte == d
+            while (hit) {
+                uint32_t b = (__ffs(hit) - 1) >> 3;
+                hit &= hit - 1;
+                uint64_t idx = ch * 16u + (uint64_t)q * 4u + b;
+                if (idx >= P.n_entries) break;
+                State s;
+                unrank_dev<MODE, NEC>(T, P.class_rep, idx, s);
+                for (int m = 0; m < 18; ++m) {
+                    State n = s;
+                    move_right(T, n, m);
+                    local += claim_with_stabilizer<MODE, NEC>(T, P, n, d + 1u);
+                }
+            }
+        }
+    }
+    add_count(P.counter, local);
+}
+
+// Backward pass: an unvisited entry with a neighbour at depth d is at depth d + 1.
+template <int MODE, int NEC>
+__global__ void __launch_bounds__(256) bfs_backward(const DevTables* __restrict__ gT, BfsParams P, uint32_t d) {
+    __shared__ DevTables T;
+    stage_tables(T, gT);
+    unsigned long long local = 0;
+    uint4* chunks = reinterpret_cast<uint4*>(P.depth);
+    for (uint64_t ch = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; ch < P.n_chunks;
+         ch += (uint64_t)gridDim.x * blockDim.x) {
+        uint4 v = chunks[ch];
+        uint32_t w[4] = {v.x, v.y, v.z, v.w};
+        bool changed = false;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uint32_t x = w[q];
+            uint32_t hit = x & (x << 1) & (x << 2) & (x << 3) & (x << 4) & (x << 5) & (x << 6) & (x << 7) &
+                           0x80808080u;  // 0x80 where byte == 0xFF
+            while (hit) {
+                uint32_t b = (__ffs(hit) - 1) >> 3;
+                hit &= hit - 1;
+                uint64_t idx = ch * 16u + (uint64_t)q * 4u + b;
+                if (idx >= P.n_entries) break;
+                State s;
+                unrank_dev<MODE, NEC>(T, P.class_rep, idx, s);
+                for (int m = 0; m < 18; ++m) {
+                    State n = s;
+                    move_right(T, n, m);
+                    uint64_t j = table_index_dev<MODE, NEC>(T, P.classidx, n);
+                    if (((volatile uint8_t*)P.depth)[j] == d) {
+                        w[q] = (w[q] & ~(0xFFu << (8 * b))) | ((d + 1u) << (8 * b));
+                        changed = true;
+                        ++local;
+                        break;
+                    }
+                }
+            }
+        }
+        if (changed) chunks[ch] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    add_count(P.counter, local);
+}
+
+// Histogram of depth values (0..31, plus unvisited in bin 32).
+__global__ void __launch_bounds__(256) bfs_histogram(const uint8_t* __restrict__ depth, uint64_t n_entries,
+                                                     unsigned long long* __restrict__ hist) {
+    __shared__ unsigned long long sh[33];
+    if (threadIdx.x < 33) sh[threadIdx.x] = 0;
+    __syncthreads();
+    uint64_t n_chunks = (n_entries + 15) / 16;
+    const uint4* chunks = reinterpret_cast<const uint4*>(depth);
+    uint32_t local[33];
+#pragma unroll
+    for (int i = 0; i < 33; ++i) local[i] = 0;
+    for (uint64_t ch = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; ch < n_chunks;
+         ch += (uint64_t)gridDim.x * blockDim.x) {
+        uint4 v = chunks[ch];
+        uint32_t w[4] = {v.x, v.y, v.z, v.w};
+        for (int q = 0; q < 16; ++q) {
+            uint64_t idx = ch * 16u + q;
+            if (idx >= n_entries) break;
+            uint32_t b = (w[q >> 2] >> (8 * (q & 3))) & 0xFFu;
+            local[b > 31u ? 32u : b] += 1u;
+        }
+    }
+    for (int i = 0; i < 33; ++i)
+        if (local[i]) atomicAdd(&sh[i], (unsigned long long)local[i]);
+    __syncthreads();
+    if (threadIdx.x < 33 && sh[threadIdx.x]) atomicAdd(&hist[threadIdx.x], sh[threadIdx.x]);
+}
+
+// 2-bit block file: per 124-entry block, u8 minimum then offsets min(depth - minimum, 3) at bit
+// 8 + 2j; entries past the end keep offset 0 (kernels.cu:396-434, 485-503).  A CTA stages 256
+// blocks (31,744 bytes = 1,984 aligned 16-byte chunks) in shared memory.
+__global__ void __launch_bounds__(256) encode_block(const uint8_t* __restrict__ depth, uint64_t n_entries,
+                                                    uint64_t n_blocks, uint32_t* __restrict__ out) {
+    __shared__ uint4 tile[1984];
+    const uint8_t* tb = reinterpret_cast<const uint8_t*>(tile);
+    for (uint64_t b0 = (uint64_t)blockIdx.x * 256u; b0 < n_blocks; b0 += (uint64_t)gridDim.x * 256u) {
+        const uint4* src = reinterpret_cast<const uint4*>(depth + b0 * 124u);
+        uint64_t avail = (n_entries + 15) / 16 - b0 * 124u / 16;  // depth array is padded to 16
+        for (int i = threadIdx.x; i < 1984; i += 256) tile[i] = (uint64_t)i < avail ? src[i] : make_uint4(~0u, ~0u, ~0u, ~0u);
+        __syncthreads();
+        uint64_t b = b0 + threadIdx.x;
+        if (b < n_blocks) {
+            uint64_t first = b * 124u;
+            uint32_t n = (uint32_t)min((uint64_t)124u, n_entries - first);
+            const uint8_t* v = tb + threadIdx.x * 124u;
+            uint32_t mn = 255;
+            for (uint32_t j = 0; j < n; ++j) mn = min(mn, (uint32_t)v[j]);
+            uint32_t words[8] = {mn, 0, 0, 0, 0, 0, 0, 0};
+            for (uint32_t j = 0; j < n; ++j) {
+                uint32_t off = min((uint32_t)v[j] - mn, 3u);
+                uint32_t pos = 8u + 2u * j;
+                words[pos >> 5] |= off << (pos & 31u);
+            }
+            uint4* o = reinterpret_cast<uint4*>(out + b * 8u);
+            o[0] = make_uint4(words[0], words[1], words[2], words[3]);
+            o[1] = make_uint4(words[4], words[5], words[6], words[7]);
+        }
+        __syncthreads();
+    }
+}
+
+// Base-3 file (kernels.cu:1839-1869).  The value of an entry is what the reference recovers from
+// its 2-bit block and mod-3 tables: exact up to the 124-block minimum + 5, otherwise the
+// smallest value >= minimum + 3 with the right residue.  Per 155-entry block: minimum m, cut
+// c in 0..3 maximising the sum of the encoded bounds (lowest c on ties), header m | c << 6, then
+// five base-3 digits per byte (least significant = first entry).
+__global__ void __launch_bounds__(128) encode_b3(const uint8_t* __restrict__ depth, const uint32_t* __restrict__ blk,
+                                                 uint64_t n_entries, uint64_t n_blocks, uint32_t* __restrict__ out) {
+    uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (b >= n_blocks) return;
+    uint64_t first = b * 155u;
+    uint32_t n = (uint32_t)min((uint64_t)155u, n_entries - first);
+    unsigned char v[155];
+    uint32_t m = 255;
+    for (uint32_t j = 0; j < n; ++j) {
+        uint64_t x = first + j;
+        uint32_t dx = depth[x];
+        uint32_t m124 = __ldg(blk + (x / 124u) * 8u) & 0xFFu;
+        uint32_t val = dx <= m124 + 5u ? dx : m124 + 3u + (dx - m124 - 3u) % 3u;
+        v[j] = (unsigned char)val;
+        m = min(m, val);
+    }
+    uint32_t best = 0, best_score = 0;
+    for (uint32_t c = 0; c < 4; ++c) {
+        uint32_t score = 0;
+        for (uint32_t j = 0; j < n; ++j) score += v[j] <= m + c ? m : (v[j] == m + c + 1 ? m + c + 1 : m + c + 2);
+        if (score > best_score) best_score = score, best = c;
+    }
+    unsigned char bytes[32];
+    bytes[0] = (unsigned char)(m | (best << 6));
+    for (uint32_t q = 0; q < 31; ++q) {
+        uint32_t x = 0;
+        for (int k = 4; k >= 0; --k) {
+            uint32_t j = q * 5u + (uint32_t)k, dg = 0;
+            if (j < n) dg = v[j] <= m + best ? 0u : (v[j] == m + best + 1 ? 1u : 2u);
+            x = x * 3u + dg;
+        }
+        bytes[1 + q] = (unsigned char)x;
+    }
+    uint32_t* o = out + b * 8u;
+    for (int w = 0; w < 8; ++w)
+        o[w] = bytes[4 * w] | (bytes[4 * w + 1] << 8) | (bytes[4 * w + 2] << 16) | ((uint32_t)bytes[4 * w + 3] << 24);
+}
+
+}  // namespace ccs

@@ -1,0 +1,249 @@
+// Device cube math for libccs: moves on packed states, the symmetry-reduced table index, table
+// decoding.  All integer; written for sm_100a.
+//
+// Index semantics follow the reference's kernels.cu:134-215 and :275-279 (corner raw coordinate,
+// class and symmetry from classidx, edge coordinate of the conjugated edges) and the block /
+// base-3 decoders of kernels.cu:396-434.  The formulation is this library's own: a U-D symmetry
+// keeps the E layer and maps the U and D layers onto themselves, so the position permutation of
+// an edge word is a single byte permute; masks are gathered with multiplies; E flips and non-E
+// flips come from one 256-entry table per word; the E-content class is read straight from the
+// 8-bit label string.
+#pragma once
+
+#include <cstdint>
+
+#include "dev_tables.h"
+
+namespace ccs {
+
+struct State {
+    uint32_t c0, c1, e0, e1, e2;
+};
+
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t s) { return __byte_perm(a, b, s); }
+
+// Corner bytes cp | o << 3 with o in 0..4 after an addition: bring o back to 0..2.  A byte is
+// >= 24 exactly when o >= 3; (byte + 8) then has bit 5 set and subtracting 0x20 - 0x08 = 0x18
+// per such byte wraps it.
+__device__ __forceinline__ uint32_t wrap_twist(uint32_t a) {
+    uint32_t t = (a + 0x08080808u) & 0x20202020u;
+    return a - t + (t >> 2);
+}
+
+// Bit b of every byte, gathered into 4 bits (byte 0 -> bit 0).
+__device__ __forceinline__ uint32_t gather4(uint32_t v, int b) {
+    return (((v >> b) & 0x01010101u) * 0x01020408u) >> 24;
+}
+
+// Low 2 bits of every byte, gathered into 8 bits (byte 0 -> bits 0-1).
+__device__ __forceinline__ uint32_t labels8(uint32_t v) { return ((v & 0x03030303u) * 0x01041040u) >> 24; }
+
+// Byte-wise values < 8 as a prmt selector (nibble j = byte j).
+__device__ __forceinline__ uint32_t nib_sel(uint32_t v) { return prmt(v | (v >> 4), 0u, 0x4420u); }
+
+__device__ __forceinline__ void move_right(const DevTables& T, State& s, int m) {
+    uint32_t a = prmt(s.c0, s.c1, T.mv_csel[m][0]) + T.mv_cadd[m][0];
+    uint32_t b = prmt(s.c0, s.c1, T.mv_csel[m][1]) + T.mv_cadd[m][1];
+    s.c0 = wrap_twist(a);
+    s.c1 = wrap_twist(b);
+    uint32_t o[3];
+#pragma unroll
+    for (int w = 0; w < 3; ++w) {
+        uint32_t x = prmt(s.e0, s.e1, T.mv_esel[m][w]);
+        uint32_t y = prmt(s.e2, s.e2, T.mv_esel2[m][w]);
+        uint32_t k = T.mv_emsk[m][w];
+        o[w] = ((x & ~k) | (y & k)) ^ T.mv_eflp[m][w];
+    }
+    s.e0 = o[0];
+    s.e1 = o[1];
+    s.e2 = o[2];
+}
+
+// s <- m * s: every cubie c (and its orientation) is renamed through the move.
+__device__ __forceinline__ void move_left(const DevTables& T, State& s, int m) {
+    const uint32_t l0 = T.lf_c[m][0], l1 = T.lf_c[m][1];
+    s.c0 = wrap_twist(prmt(l0, l1, nib_sel(s.c0 & 0x07070707u)) + (s.c0 & 0x18181818u));
+    s.c1 = wrap_twist(prmt(l0, l1, nib_sel(s.c1 & 0x07070707u)) + (s.c1 & 0x18181818u));
+    const uint32_t r0 = T.lf_e[m][0], r1 = T.lf_e[m][1], r2 = T.lf_e[m][2];
+    uint32_t e[3] = {s.e0, s.e1, s.e2};
+#pragma unroll
+    for (int w = 0; w < 3; ++w) {
+        uint32_t v = e[w];
+        uint32_t sel = nib_sel(v & 0x07070707u);
+        uint32_t hi = ((v >> 3) & 0x01010101u) * 0xFFu;  // cubies 8..11 rename through r2
+        e[w] = ((prmt(r0, r1, sel) & ~hi) | (prmt(r2, r2, sel) & hi)) ^ (v & 0x10101010u);
+    }
+    s.e0 = e[0];
+    s.e1 = e[1];
+    s.e2 = e[2];
+}
+
+__device__ __forceinline__ uint32_t corner_raw_dev(const DevTables& T, const State& s) {
+    uint32_t olo = (s.c0 >> 3) & 0x03030303u;
+    uint32_t ohi = (s.c1 >> 3) & 0x00030303u;
+    uint32_t twist = __dp4a(olo, 0x1B090301u, 0u) + 81u * __dp4a(ohi, 0x00090301u, 0u);
+    uint32_t dmask = gather4(s.c0, 2) | (gather4(s.c1, 2) << 4);
+    return twist * 70u + T.ccomb_rank[dmask];
+}
+
+// Edges conjugated by U-D symmetry sym.
+__device__ __forceinline__ void conj_edges(const DevTables& T, const State& s, int sym, uint32_t e[3]) {
+    uint32_t p[3];
+    p[0] = prmt(s.e0, s.e1, T.sy_psel[sym][0]);
+    p[1] = prmt(s.e0, s.e1, T.sy_psel[sym][1]);
+    p[2] = prmt(s.e2, s.e2, T.sy_psel[sym][2]);
+    const uint32_t r0 = T.sy_rel[sym][0], r1 = T.sy_rel[sym][1], r2 = T.sy_rel[sym][2];
+#pragma unroll
+    for (int w = 0; w < 3; ++w) {
+        uint32_t v = p[w];
+        uint32_t sel = nib_sel(v & 0x07070707u);
+        uint32_t hi = ((v >> 3) & 0x01010101u) * 0xFFu;
+        e[w] = ((prmt(r0, r1, sel) & ~hi) | (prmt(r2, r2, sel) & hi)) ^ (v & 0x10101010u) ^ T.sy_pflp[sym][w];
+    }
+}
+
+// Edge coordinate of conjugated edges e.  MODE KIND_GEN: (slice * 256 + non-E flips) * NEC +
+// class of the E content; KIND_304: (slice * 70 + U layout of the non-E positions) * 16 + E flips.
+template <int MODE, int NEC>
+__device__ __forceinline__ uint32_t edge_coord_dev(const DevTables& T, const uint32_t e[3]) {
+    uint32_t em0 = gather4(e[0], 3), em1 = gather4(e[1], 3), em2 = gather4(e[2], 3);
+    uint32_t om0 = gather4(e[0], 4), om1 = gather4(e[1], 4), om2 = gather4(e[2], 4);
+    uint32_t n0 = __popc(em0), n1 = __popc(em1);
+    uint32_t f0 = T.flp[(em0 << 4) | om0], f1 = T.flp[(em1 << 4) | om1], f2 = T.flp[(em2 << 4) | om2];
+    uint32_t eflips = (f0 & 15u) | ((f1 & 15u) << n0) | ((f2 & 15u) << (n0 + n1));
+    uint32_t slice = T.slice_rank[em0 | (em1 << 4) | (em2 << 8)];
+    if (MODE == KIND_304) {
+        uint32_t um0 = gather4(~(e[0] | (e[0] >> 1)), 2), um1 = gather4(~(e[1] | (e[1] >> 1)), 2),
+                 um2 = gather4(~(e[2] | (e[2] >> 1)), 2);
+        uint32_t u = T.ump[(em0 << 4) | um0] | (T.ump[(em1 << 4) | um1] << (4 - n0)) |
+                     (T.ump[(em2 << 4) | um2] << (8 - n0 - n1));
+        return (slice * 70u + T.ccomb_rank[u]) * 16u + eflips;
+    } else {
+        uint32_t nflips = (f0 >> 4) | ((f1 >> 4) << (4 - n0)) | ((f2 >> 4) << (8 - n0 - n1));
+        uint32_t eord = T.cmp4[em0][labels8(e[0])] | ((uint32_t)T.cmp4[em1][labels8(e[1])] << (2 * n0)) |
+                        ((uint32_t)T.cmp4[em2][labels8(e[2])] << (2 * (n0 + n1)));
+        return (slice * 256u + nflips) * (uint32_t)NEC + T.genc[(eord << 4) | eflips];
+    }
+}
+
+template <int MODE, int NEC>
+struct KindTraits {
+    static constexpr uint64_t N_EDGE = MODE == KIND_304 ? 495ull * 70ull * 16ull : 495ull * 256ull * (uint64_t)NEC;
+};
+
+template <int MODE, int NEC>
+__device__ __forceinline__ uint64_t table_index_dev(const DevTables& T, const uint32_t* __restrict__ classidx,
+                                                    const State& s) {
+    uint32_t packed = __ldg(classidx + corner_raw_dev(T, s));
+    uint32_t e[3];
+    conj_edges(T, s, packed & 15u, e);
+    return (uint64_t)(packed >> 4) * KindTraits<MODE, NEC>::N_EDGE + edge_coord_dev<MODE, NEC>(T, e);
+}
+
+// Table formats.
+enum Format : int { FMT_BLOCK = 0, FMT_B3 = 1 };
+
+// Lower bound of entry idx.  Block: per 32-byte sector a u8 minimum then 124 two-bit offsets
+// (3 = at least minimum + 3) starting at bit 8.  Base 3: header m | cut << 6, then 155 digits,
+// five per byte (digit 0 = at least m, 1 = m + cut + 1, 2 = at least m + cut + 2).
+template <int FMT>
+__device__ __forceinline__ uint32_t lower_bound_dev(const uint32_t* __restrict__ tab, uint64_t idx) {
+    if (FMT == FMT_B3) {
+        uint64_t b = idx / 155u;
+        uint32_t j = (uint32_t)(idx - b * 155u);
+        const unsigned char* p = reinterpret_cast<const unsigned char*>(tab) + b * 32u;
+        uint32_t hdr = __ldg(p), byte = __ldg(p + 1u + j / 5u);
+        uint32_t k = j % 5u;
+        uint32_t pw = k == 0 ? 1u : k == 1 ? 3u : k == 2 ? 9u : k == 3 ? 27u : 81u;
+        uint32_t d = (byte / pw) % 3u;
+        uint32_t m = hdr & 63u;
+        return d == 0u ? m : m + (hdr >> 6) + d;
+    } else {
+        uint64_t b = idx / 124u;
+        uint32_t pos = 8u + 2u * (uint32_t)(idx - b * 124u);
+        const uint32_t* p = tab + b * 8u;
+        return (__ldg(p) & 0xFFu) + ((__ldg(p + (pos >> 5)) >> (pos & 31u)) & 3u);
+    }
+}
+
+__device__ __forceinline__ bool is_solved(const State& s) {
+    return s.c0 == 0x03020100u && s.c1 == 0x07060504u && s.e0 == 0x03020100u && s.e1 == 0x07060504u &&
+           s.e2 == 0x0B0A0908u;
+}
+
+// Representative state of entry idx (the BFS expands it): corners from the class
+// representative's raw coordinate, edges from the edge coordinate.  Follows kernels.cu:294-379.
+template <int MODE, int NEC>
+__device__ __forceinline__ void unrank_dev(const DevTables& T, const uint32_t* __restrict__ class_rep, uint64_t idx,
+                                           State& s) {
+    constexpr uint64_t NE = KindTraits<MODE, NEC>::N_EDGE;
+    uint32_t cls = (uint32_t)(idx / NE);
+    uint32_t coord = (uint32_t)(idx - (uint64_t)cls * NE);
+    uint32_t raw = __ldg(class_rep + cls);
+    uint32_t twist = raw / 70u;
+    uint32_t dmask = T.ccomb_unrank[raw - twist * 70u];
+    uint32_t c[8];
+    uint32_t osum = 0, nu = 0, nd = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        uint32_t o;
+        if (i < 7) {
+            o = twist % 3u;
+            twist /= 3u;
+            osum += o;
+        } else {
+            o = (3u - osum % 3u) % 3u;
+        }
+        uint32_t cp = (dmask >> i) & 1u ? 4u + nd++ : nu++;
+        c[i] = cp | (o << 3);
+    }
+    s.c0 = c[0] | (c[1] << 8) | (c[2] << 16) | (c[3] << 24);
+    s.c1 = c[4] | (c[5] << 8) | (c[6] << 16) | (c[7] << 24);
+    uint32_t emask, eord, eflips, umask, nflips;
+    if (MODE == KIND_304) {
+        uint32_t ef = coord % 16u, rest = coord / 16u;
+        uint32_t u = rest % 70u;
+        emask = T.slice_unrank[rest / 70u];
+        eord = 0xE4u;
+        eflips = ef;
+        umask = T.ccomb_unrank[u];
+        nflips = 0;
+    } else {
+        uint32_t gc = coord % (uint32_t)NEC, grest = coord / (uint32_t)NEC;
+        nflips = grest % 256u;
+        emask = T.slice_unrank[grest / 256u];
+        uint32_t content = T.gen_rep[__popc(nflips) & 1u][gc];
+        eord = T.eorder_unrank[content >> 4];
+        eflips = content & 15u;
+        umask = 0x0Fu;
+    }
+    uint32_t e[3] = {0, 0, 0};
+    uint32_t ne = 0, no = 0, nue = 0, nde = 0;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        uint32_t b, flip;
+        if ((emask >> i) & 1u) {
+            b = 8u | ((eord >> (2 * ne)) & 3u);
+            flip = (eflips >> ne) & 1u;
+            ++ne;
+        } else {
+            b = (umask >> no) & 1u ? nue++ : 4u + nde++;
+            flip = (nflips >> no) & 1u;
+            ++no;
+        }
+        e[i >> 2] |= (b | (flip << 4)) << ((i & 3) * 8);
+    }
+    s.e0 = e[0];
+    s.e1 = e[1];
+    s.e2 = e[2];
+}
+
+// Copy the constant tables into shared memory (whole block).
+__device__ __forceinline__ void stage_tables(DevTables& dst, const DevTables* __restrict__ src) {
+    const uint4* s = reinterpret_cast<const uint4*>(src);
+    uint4* d = reinterpret_cast<uint4*>(&dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(DevTables) / 16); i += blockDim.x) d[i] = s[i];
+    __syncthreads();
+}
+
+}  // namespace ccs

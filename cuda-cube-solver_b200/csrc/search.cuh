@@ -1,0 +1,65 @@
+// Device-side data of the IDA* search: cube slots, the work ring, launch parameters.
+#pragma once
+
+#include <cstdint>
+
+namespace ccs {
+
+constexpr uint32_t SLOT_FREE = 0, SLOT_ACTIVE = 1, SLOT_SOLVED = 2, SLOT_ERROR = 3;
+constexpr unsigned long long TICKET_IDLE = 0x7FFFFFFFull;  // ticket of a slot with no iteration: exhausted
+constexpr int MAX_PLEN = 6;
+constexpr uint32_t MAX_BOUND = 22;   // every position is solvable in 20 half-turn moves
+
+// One cube under search.  The ticket is the work counter of the current IDA* iteration
+// ("epoch"): plen << 56 | bound << 48 | epoch << 32 | next item index; one atomicAdd hands out
+// an item together with the bound and prefix length it belongs to.
+struct alignas(16) Slot {
+    uint32_t frame[30];              // root frames: g, R g R^-1, R^2 g R^-2, then their inverses
+    uint32_t h0;                     // root lower bounds, 5 bits per frame
+    uint32_t status;
+    unsigned long long ticket;
+    uint32_t done;                   // items finished in the current epoch
+    uint32_t found;                  // set by the first lane that finds a solution
+    uint32_t sol_len;
+    uint32_t request;                // caller's tag (server request id)
+    uint8_t sol[24];
+    unsigned long long nodes, probes;
+    unsigned long long iter_nodes[24];  // nodes per bound
+    unsigned long long t_admit, t_done; // device globaltimer, ns
+};
+
+struct QueueState {
+    unsigned long long head, tail;   // ring positions, monotonic
+    uint32_t active;                 // cubes admitted and not finished
+    uint32_t error;                  // error bits (ERR_*)
+    unsigned long long probes;       // table probes done by all lanes
+    unsigned long long steps;        // lane steps (diagnostic)
+    unsigned long long finished;     // cubes finished (monotonic)
+    unsigned long long admit_head;   // admission ring: cubes waiting for a first iteration
+    unsigned long long admit_tail;
+    uint32_t yield;                  // host asks lanes to stop fetching new items
+    uint32_t pad;
+};
+
+constexpr uint32_t ERR_IDLE_LIMIT = 1u, ERR_BOUND = 2u, ERR_STACK = 4u;
+
+struct SearchParams {
+    Slot* slots;
+    QueueState* q;
+    unsigned long long* ring;        // entries: lap << 32 | slot
+    uint32_t ring_cap;
+    unsigned long long* admit;       // admission entries: lap << 32 | slot
+    uint32_t admit_cap;
+    uint32_t n_slots;
+    const uint32_t* classidx;
+    const uint32_t* table;           // solving table (block or base 3)
+    const uint32_t* prefixes[MAX_PLEN + 1];  // canonical move sequences, 5 bits per move
+    uint32_t n_prefix[MAX_PLEN + 1];
+    uint32_t base_plen;              // prefix length of a cube's first iterations
+    unsigned long long deeper_at[2]; // an iteration of at least this many nodes -> one move longer
+    uint32_t idle_limit;             // idle polls before a warp leaves (kernel relaunched by the host)
+    unsigned long long* done_log;    // host-mapped completion log (server), may be null
+    uint32_t done_log_cap;
+};
+
+}  // namespace ccs

@@ -1,0 +1,376 @@
+// The IDA* search kernel (persistent, continuous batching).
+//
+// Method (the reference's, kernels.cu:644-1801 and solver.py:254-320): IDA* over six frames of
+// the cube -- g conjugated so each of its three axes becomes the U-D axis, and the inverses of
+// those three -- with one lower bound per frame from the coset table; a child is pruned when
+// g + 1 + bound > threshold; the coset axis rule excludes first moves on an axis whose inverse
+// frame is tight, and prunes a child whose three forward (or three inverse) frames are all
+// tight; an inverse frame on the move's own axis keeps its parent's value (same coset); frames
+// are probed at the budget edge first, one below next, the rest last.
+//
+// Execution (this library's own): every lane runs its own depth-first search over one work item
+// (a cube and a canonical move prefix).  Per warp iteration each lane performs exactly one table
+// probe; control work (next child, push, pop, item fetch) runs between probes.  Work comes from
+// a device ring of cube slots: the ticket of a slot hands out the prefix items of its current
+// iteration, and the lane that finishes the last item of an iteration either records the
+// solution or publishes the next iteration (bound + 1) and re-queues the slot, so a batch of
+// cubes advances with no host round trip per bound.  Waits are bounded: a warp with nothing to
+// do polls a limited number of times and then leaves; the host relaunches while cubes remain.
+#pragma once
+
+#include "cube_dev.cuh"
+#include "search.cuh"
+
+namespace ccs {
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ uint32_t hget(uint32_t h, int k) { return (h >> (5 * k)) & 31u; }
+__device__ __forceinline__ uint32_t hset(uint32_t h, int k, uint32_t v) {
+    return (h & ~(31u << (5 * k))) | (v << (5 * k));
+}
+__device__ __forceinline__ uint32_t hrep(uint32_t v) { return v * 0x2108421u; }  // v in all six fields
+
+// Axes (bit a: moves of faces a and a + 3) on which the next move may not lie: inverse frame
+// 3 + a is tight, so no solution of exactly this length starts with a turn on axis a.
+__device__ __forceinline__ uint32_t excluded_axes(uint32_t h, uint32_t budget) {
+    uint32_t x = h ^ hrep(budget);
+    return (uint32_t)(((x >> 15) & 31u) == 0u) | ((uint32_t)(((x >> 20) & 31u) == 0u) << 1) |
+           ((uint32_t)(((x >> 25) & 31u) == 0u) << 2);
+}
+
+__device__ __forceinline__ uint32_t axis_move_mask(uint32_t axes) {
+    return ((axes & 1u) ? 0x00E07u : 0u) | ((axes & 2u) ? 0x07038u : 0u) | ((axes & 4u) ? 0x381C0u : 0u);
+}
+
+// All three forward frames (or all three inverse frames) tight: no last (first) move possible.
+__device__ __forceinline__ bool all_axes_tight(uint32_t c, uint32_t budget) {
+    if (budget == 0u) return false;
+    uint32_t x = c ^ hrep(budget);
+    return (x & 0x7FFFu) == 0u || ((x >> 15) & 0x7FFFu) == 0u;
+}
+
+// Probe order masks: frames at the budget edge | one below << 6 | the rest << 12.
+__device__ __forceinline__ uint32_t frame_order(uint32_t h, uint32_t edge) {
+    uint32_t at = 0, below = 0;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        uint32_t v = hget(h, j);
+        at |= (uint32_t)(v >= edge) << j;
+        below |= (uint32_t)(v + 1u == edge) << j;
+    }
+    return at | (below << 6) | ((~(at | below) & 0x3Fu) << 12);
+}
+
+__device__ __forceinline__ int next_frame(uint32_t& rem) {
+    if (!rem) return 6;
+    int b = __ffs(rem) - 1;
+    rem &= rem - 1;
+    return b % 6;
+}
+
+__device__ __forceinline__ void frame_do(const DevTables& T, State& f, int k, int m) {
+    if (k < 3) move_right(T, f, T.frame_move[k][m]);
+    else move_left(T, f, T.inv_move[T.frame_move[k - 3][m]]);
+}
+
+__device__ __forceinline__ void frame_undo(const DevTables& T, State& f, int k, int m) {
+    if (k < 3) move_right(T, f, T.inv_move[T.frame_move[k][m]]);
+    else move_left(T, f, T.frame_move[k - 3][m]);
+}
+
+__device__ __forceinline__ uint64_t ticket_make(uint32_t plen, uint32_t bound, uint32_t epoch) {
+    return ((uint64_t)plen << 56) | ((uint64_t)bound << 48) | ((uint64_t)(epoch & 0xFFFFu) << 32);
+}
+
+__device__ __forceinline__ void enqueue_slot(const SearchParams& P, uint32_t s) {
+    unsigned long long pos = atomicAdd(&P.q->tail, 1ull);
+    unsigned long long lap = pos / P.ring_cap;
+    atomicExch(&P.ring[pos % P.ring_cap], (lap << 32) | s);
+}
+
+__device__ __forceinline__ void publish_epoch(const SearchParams& P, uint32_t s, uint32_t plen, uint32_t bound,
+                                              uint32_t epoch) {
+    Slot& sl = P.slots[s];
+    sl.done = 0;
+    __threadfence();
+    atomicExch(&sl.ticket, ticket_make(plen, bound, epoch));
+    __threadfence();
+    enqueue_slot(P, s);
+}
+
+__device__ __forceinline__ void finish_slot(const SearchParams& P, uint32_t s, uint32_t status) {
+    Slot& sl = P.slots[s];
+    sl.t_done = globaltimer_ns();
+    __threadfence();
+    atomicExch(&sl.status, status);
+    __threadfence();
+    if (P.done_log) {
+        unsigned long long k = atomicAdd(&P.q->finished, 1ull);
+        volatile unsigned long long* log = P.done_log;
+        log[k % P.done_log_cap] = ((unsigned long long)(k / P.done_log_cap + 1) << 32) | s;
+        __threadfence_system();
+    } else {
+        atomicAdd(&P.q->finished, 1ull);
+    }
+    atomicSub(&P.q->active, 1u);
+}
+
+// Prefix length of the next iteration: base, plus one per threshold the last iteration reached
+// (a few huge subtrees would otherwise leave the GPU idle), at most the bound.
+__device__ __forceinline__ uint32_t next_plen(const SearchParams& P, unsigned long long last_nodes, uint32_t bound) {
+    uint32_t pl = P.base_plen + (last_nodes >= P.deeper_at[0]) + (last_nodes >= P.deeper_at[1]);
+    pl = pl > (uint32_t)MAX_PLEN ? (uint32_t)MAX_PLEN : pl;
+    return pl < bound ? pl : bound;
+}
+
+enum FetchResult { FETCH_OK = 0, FETCH_EMPTY = 1, FETCH_FINISHED = 2, FETCH_ADMIT = 3 };
+
+// Next unit of work for a lane: a cube to admit (admission ring, first), or a prefix item of a
+// queued iteration (work ring).  FETCH_FINISHED when nothing is queued, admitted or in flight.
+__device__ __forceinline__ int fetch_item(const SearchParams& P, uint32_t& slot, uint32_t& idx, uint32_t& plen,
+                                          uint32_t& bound, uint32_t& epoch) {
+    volatile QueueState* q = P.q;
+    for (int tries = 0; tries < 64; ++tries) {
+        if (q->yield) return FETCH_FINISHED;  // the host is stopping this launch
+        unsigned long long ah = q->admit_head;
+        if (ah < q->admit_tail) {
+            unsigned long long e = ((volatile unsigned long long*)P.admit)[ah % P.admit_cap];
+            if ((e >> 32) != ah / P.admit_cap) return FETCH_EMPTY;  // reserved, not yet written
+            atomicAdd(&P.q->active, 1u);  // counted before the entry leaves the ring
+            if (atomicCAS((unsigned long long*)&P.q->admit_head, ah, ah + 1) == ah) {
+                slot = (uint32_t)e;
+                return FETCH_ADMIT;
+            }
+            atomicSub(&P.q->active, 1u);
+            continue;
+        }
+        unsigned long long h = q->head, t = q->tail;
+        if (h >= t) return (q->active == 0u && q->admit_head >= q->admit_tail) ? FETCH_FINISHED : FETCH_EMPTY;
+        unsigned long long e = ((volatile unsigned long long*)P.ring)[h % P.ring_cap];
+        if ((e >> 32) != h / P.ring_cap) return FETCH_EMPTY;  // reserved, not yet written
+        uint32_t s = (uint32_t)e;
+        unsigned long long tk = atomicAdd(&P.slots[s].ticket, 1ull);
+        uint32_t i = (uint32_t)tk, pl = (uint32_t)(tk >> 56);
+        if (pl <= (uint32_t)MAX_PLEN && i < P.n_prefix[pl]) {
+            slot = s;
+            idx = i;
+            plen = pl;
+            bound = (uint32_t)(tk >> 48) & 0xFFu;
+            epoch = (uint32_t)(tk >> 32) & 0xFFFFu;
+            return FETCH_OK;
+        }
+        atomicCAS((unsigned long long*)&P.q->head, h, h + 1);  // this entry's iteration is handed out
+    }
+    return FETCH_EMPTY;
+}
+
+template <int MODE, int NEC, int FMT>
+__device__ __forceinline__ uint32_t probe_bound(const DevTables& T, const SearchParams& P, const State& s) {
+    return lower_bound_dev<FMT>(P.table, table_index_dev<MODE, NEC>(T, P.classidx, s));
+}
+
+// Admission of a new cube: root bounds of its six frames, first threshold, first iteration.
+template <int MODE, int NEC, int FMT>
+__device__ void admit_slot(const DevTables& T, const SearchParams& P, uint32_t s) {
+    Slot& sl = P.slots[s];
+    State f0{sl.frame[0], sl.frame[1], sl.frame[2], sl.frame[3], sl.frame[4]};
+    uint32_t h = 0, bound = 0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        State f{sl.frame[5 * k], sl.frame[5 * k + 1], sl.frame[5 * k + 2], sl.frame[5 * k + 3], sl.frame[5 * k + 4]};
+        uint32_t v = probe_bound<MODE, NEC, FMT>(T, P, f);
+        v = v > 31u ? 31u : v;
+        h = hset(h, k, v);
+        bound = v > bound ? v : bound;
+    }
+    atomicAdd(&sl.probes, 6ull);
+    atomicAdd(&P.q->probes, 6ull);
+    sl.h0 = h;
+    sl.t_admit = globaltimer_ns();
+    if (is_solved(f0)) {
+        sl.sol_len = 0;
+        sl.found = 1;
+        finish_slot(P, s, SLOT_SOLVED);
+        return;
+    }
+    if (bound == 0u) bound = 1u;  // not solved, so at least one move
+    publish_epoch(P, s, next_plen(P, 0ull, bound), bound, 1u);
+}
+
+template <int MODE, int NEC, int FMT, int THREADS>
+__global__ void __launch_bounds__(THREADS) search_kernel(const DevTables* __restrict__ gT, SearchParams P) {
+    __shared__ DevTables T;
+    stage_tables(T, gT);
+
+    unsigned char path[MAX_DEPTH];
+    uint32_t hstack[MAX_DEPTH];
+    State f[6];
+    uint32_t h = 0, c = 0;        // packed bounds of the node and of the child under evaluation
+    uint32_t slot = 0, idx = 0, plen = 0, bound = 0, epoch = 0, pseq = 0;
+    int g = 0, last = -1, m = -1, k = 0;
+    uint32_t todo = 0, ord = 0, rem = 0;
+    unsigned long long nodes = 0, probes = 0;
+    bool have_item = false, done = false, idle = false;
+    uint32_t iter = 0, idle_polls = 0, backoff = 32;
+    const uint32_t lane = threadIdx.x & 31u;
+
+    for (;;) {
+        bool eval = false;
+        idle = false;
+        // ---- control: until this lane has a child frame to probe (or nothing to do) ----
+        while (!done) {
+            if (m >= 0) {
+                if (k < 6) {  // child m still has frames to probe
+                    eval = true;
+                    break;
+                }
+                if (k == 6 && !all_axes_tight(c, bound - (uint32_t)g - 1u)) {  // push the surviving child
+#pragma unroll
+                    for (int j = 0; j < 6; ++j) frame_do(T, f[j], j, m);
+                    hstack[g] = h;
+                    path[g] = (unsigned char)m;
+                    h = c;
+                    last = m;
+                    ++g;
+                    if ((uint32_t)g == bound) {
+                        Slot& sl = P.slots[slot];
+                        if (is_solved(f[0]) && atomicCAS(&sl.found, 0u, 1u) == 0u) {
+                            sl.sol_len = (uint32_t)g;
+                            for (int j = 0; j < g; ++j) sl.sol[j] = path[j];
+                        }
+                        todo = 0;
+                    } else {
+                        uint32_t allow = (uint32_t)g < plen ? 1u << ((pseq >> (5 * g)) & 31u) : T.amask[m + 1];
+                        todo = allow & ~axis_move_mask(excluded_axes(h, bound - (uint32_t)g));
+                        ord = frame_order(h, bound - (uint32_t)g);
+                    }
+                }
+                m = -1;
+                continue;
+            }
+            if (!have_item) {
+                int r = fetch_item(P, slot, idx, plen, bound, epoch);
+                if (r == FETCH_FINISHED) {
+                    done = true;
+                    break;
+                }
+                if (r == FETCH_EMPTY) {
+                    idle = true;
+                    break;
+                }
+                if (r == FETCH_ADMIT) {
+                    admit_slot<MODE, NEC, FMT>(T, P, slot);
+                    continue;
+                }
+                Slot& sl = P.slots[slot];
+                if (*(volatile uint32_t*)&sl.found) {  // solved by another item: skip
+                    __threadfence();
+                    uint32_t d = atomicAdd(&sl.done, 1u) + 1u;
+                    if (d == P.n_prefix[plen]) finish_slot(P, slot, SLOT_SOLVED);
+                    continue;
+                }
+#pragma unroll
+                for (int j = 0; j < 6; ++j)
+                    f[j] = State{sl.frame[5 * j], sl.frame[5 * j + 1], sl.frame[5 * j + 2], sl.frame[5 * j + 3],
+                                 sl.frame[5 * j + 4]};
+                h = sl.h0;
+                pseq = plen ? __ldg(P.prefixes[plen] + idx) : 0u;
+                g = 0;
+                last = -1;
+                nodes = 0;
+                probes = 0;
+                uint32_t allow = plen ? 1u << (pseq & 31u) : T.amask[0];
+                todo = allow & ~axis_move_mask(excluded_axes(h, bound));
+                ord = frame_order(h, bound);
+                have_item = true;
+                continue;
+            }
+            if ((++iter & 1023u) == 0u &&
+                (*(volatile uint32_t*)&P.slots[slot].found || ((volatile QueueState*)P.q)->yield))
+                todo = 0, g = 0;  // solved elsewhere, or the host is stopping: drop the rest of the item
+            if (todo) {
+                m = __ffs(todo) - 1;
+                todo &= todo - 1;
+                ++nodes;
+                int inherit = 3 + (m / 3) % 3;  // inverse frame on the move's axis: same coset
+                c = h;
+                rem = ord & ~(0x41041u << inherit);
+                k = next_frame(rem);
+                eval = true;
+                break;
+            }
+            // node exhausted (or the cube was solved elsewhere): pop, or finish the item
+            if (g == 0) {
+                Slot& sl = P.slots[slot];
+                atomicAdd(&sl.nodes, nodes);
+                atomicAdd(&sl.probes, probes);
+                atomicAdd(&sl.iter_nodes[bound < 24u ? bound : 23u], nodes);
+                atomicAdd(&P.q->probes, probes);
+                __threadfence();
+                uint32_t d = atomicAdd(&sl.done, 1u) + 1u;
+                if (d == P.n_prefix[plen]) {
+                    __threadfence();
+                    if (*(volatile uint32_t*)&sl.found) {
+                        finish_slot(P, slot, SLOT_SOLVED);
+                    } else if (bound + 1u > MAX_BOUND) {
+                        atomicOr(&P.q->error, ERR_BOUND);
+                        finish_slot(P, slot, SLOT_ERROR);
+                    } else {
+                        unsigned long long last_nodes = *(volatile unsigned long long*)&sl.iter_nodes[bound];
+                        publish_epoch(P, slot, next_plen(P, last_nodes, bound + 1u), bound + 1u, epoch + 1u);
+                    }
+                }
+                have_item = false;
+                continue;
+            }
+            --g;
+            int pm = path[g];
+#pragma unroll
+            for (int j = 0; j < 6; ++j) frame_undo(T, f[j], j, pm);
+            h = hstack[g];
+            last = g > 0 ? path[g - 1] : -1;
+            todo = (uint32_t)g < plen ? 0u
+                                      : T.amask[last + 1] & ~axis_move_mask(excluded_axes(h, bound - (uint32_t)g)) &
+                                            ~((2u << pm) - 1u);
+            ord = frame_order(h, bound - (uint32_t)g);
+        }
+        if (__all_sync(0xFFFFFFFFu, done)) break;
+        // After the control phase every lane is probing, idle (no work queued) or done.
+        if (__ballot_sync(0xFFFFFFFFu, eval) == 0u) {
+            // No lane has a probe: the warp backs off; after too many empty polls in a row it
+            // leaves (warp-uniform counter), and the host relaunches while cubes remain.
+            if (++idle_polls > P.idle_limit) {
+                if (lane == 0) atomicOr(&P.q->error, ERR_IDLE_LIMIT);
+                break;
+            }
+            __nanosleep(backoff);
+            backoff = backoff < 4096u ? backoff * 2u : 4096u;
+            continue;
+        }
+        idle_polls = 0;
+        backoff = 32;
+        if (!eval) continue;
+
+        // ---- one probe: frame k of child m ----
+        State t = f[0];
+#pragma unroll
+        for (int j = 1; j < 6; ++j)
+            if (k == j) t = f[j];
+        if (k < 3) move_right(T, t, T.frame_move[k][m]);
+        else move_left(T, t, T.inv_move[T.frame_move[k - 3][m]]);
+        uint32_t v = probe_bound<MODE, NEC, FMT>(T, P, t);
+        ++probes;
+        uint32_t parent = hget(h, k);
+        if (k < 3 && parent) v = max(v, parent - 1u);  // a right move changes the coset distance by <= 1
+        v = v > 31u ? 31u : v;
+        c = hset(c, k, v);
+        k = ((uint32_t)g + 1u + v > bound) ? 7 : next_frame(rem);
+    }
+}
+
+}  // namespace ccs

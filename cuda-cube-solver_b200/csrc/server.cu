@@ -1,0 +1,233 @@
+// libccs: continuous-batching server.
+//
+// A service thread owns the search buffers of the handle.  Submitted cubes wait in a host queue
+// until a slot is free; the thread writes the slot and an admission-ring entry into device memory
+// on a copy stream while the persistent search kernel keeps running on the compute stream, so a
+// new cube starts as soon as a lane picks its admission up, next to the cubes already searching.
+// Lanes record finished slots in a host-mapped completion log; the thread reads the slot back,
+// frees it and hands the result to ccs_server_poll.  The kernel leaves when it runs out of work
+// (or after a bounded idle wait) and the thread relaunches it when cubes are in flight.
+#include <cuda_runtime.h>
+
+#include <array>
+#include <chrono>
+#include <cstring>
+#include <deque>
+#include <utility>
+#include <vector>
+
+#include "ccs_internal.h"
+#include "search_kernel.cuh"
+
+using namespace ccs;
+
+namespace ccs {
+void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P);
+int grid_for(ccs_handle* h, const ccs_solve_opts* o);
+int launch_kernel(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream);
+void make_slot(const uint32_t state[5], uint32_t request, Slot* s);
+void fill_result(const Slot& s, ccs_result* r);
+
+struct Server {
+    ccs_handle* h = nullptr;
+    ccs_solve_opts opts{};
+    uint32_t n_slots = 0;
+    cudaStream_t copy = nullptr;
+    cudaEvent_t kernel_done = nullptr;
+    bool kernel_running = false;
+    SearchParams P{};
+    int grid = 0;
+    unsigned long long* done_log = nullptr;  // host-mapped
+    unsigned long long* d_done_log = nullptr;
+    uint32_t log_cap = 0;
+    unsigned long long consumed = 0;
+    unsigned long long admit_pos = 0;
+    std::vector<uint32_t> free_slots;
+    std::vector<uint64_t> slot_request;
+    uint32_t in_flight = 0;
+
+    std::mutex mu;
+    std::condition_variable cv;
+    bool stop = false;
+    int error = CCS_OK;
+    std::string error_msg;
+    uint64_t next_id = 1;
+    std::deque<std::pair<uint64_t, std::array<uint32_t, 5>>> pending;
+    std::deque<std::pair<uint64_t, ccs_result>> finished;
+    std::thread thread;
+
+    int step();
+    void run();
+};
+
+int Server::step() {
+    // 1. completions
+    for (;;) {
+        unsigned long long e = ((volatile unsigned long long*)done_log)[consumed % log_cap];
+        if ((e >> 32) != consumed / log_cap + 1) break;
+        uint32_t s = (uint32_t)e;
+        Slot sl;
+        CCS_CUDA_TRY(cudaMemcpyAsync(&sl, h->d_slots + s, sizeof sl, cudaMemcpyDeviceToHost, copy));
+        CCS_CUDA_TRY(cudaStreamSynchronize(copy));
+        ccs_result r;
+        fill_result(sl, &r);
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            finished.emplace_back(slot_request[s], r);
+        }
+        free_slots.push_back(s);
+        --in_flight;
+        ++consumed;
+    }
+    // 2. admissions
+    std::vector<std::pair<uint64_t, std::array<uint32_t, 5>>> take;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        while (!pending.empty() && take.size() < free_slots.size()) {
+            take.push_back(pending.front());
+            pending.pop_front();
+        }
+    }
+    if (!take.empty()) {
+        for (auto& t : take) {
+            uint32_t s = free_slots.back();
+            free_slots.pop_back();
+            slot_request[s] = t.first;
+            Slot sl;
+            make_slot(t.second.data(), (uint32_t)t.first, &sl);
+            CCS_CUDA_TRY(cudaMemcpyAsync(h->d_slots + s, &sl, sizeof sl, cudaMemcpyHostToDevice, copy));
+            unsigned long long pos = admit_pos++;
+            unsigned long long entry = ((pos / P.admit_cap) << 32) | s;
+            CCS_CUDA_TRY(cudaMemcpyAsync(P.admit + pos % P.admit_cap, &entry, 8, cudaMemcpyHostToDevice, copy));
+            CCS_CUDA_TRY(cudaStreamSynchronize(copy));  // slot and entry land before the tail moves
+            ++in_flight;
+        }
+        unsigned long long tail = admit_pos;
+        CCS_CUDA_TRY(cudaMemcpyAsync(&h->d_q->admit_tail, &tail, 8, cudaMemcpyHostToDevice, copy));
+        CCS_CUDA_TRY(cudaStreamSynchronize(copy));
+    }
+    // 3. keep a search launch running while cubes are in flight
+    if (kernel_running && cudaEventQuery(kernel_done) == cudaSuccess) kernel_running = false;
+    if (!kernel_running && in_flight > 0) {
+        CCS_TRY(launch_kernel(h, P, grid, h->stream));
+        CCS_CUDA_TRY(cudaEventRecord(kernel_done, h->stream));
+        kernel_running = true;
+    }
+    return CCS_OK;
+}
+
+void Server::run() {
+    while (true) {
+        {
+            std::unique_lock<std::mutex> lock(mu);
+            if (stop) break;
+            if (pending.empty() && in_flight == 0) cv.wait_for(lock, std::chrono::milliseconds(2));
+            if (stop) break;
+        }
+        int rc = step();
+        if (rc != CCS_OK) {
+            std::lock_guard<std::mutex> lock(mu);
+            error = rc;
+            error_msg = g_last_error;
+            stop = true;
+            break;
+        }
+        if (in_flight > 0) std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+int server_stop(ccs_handle* h) {
+    Server* s = h->server;
+    if (!s) return CCS_OK;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    if (s->thread.joinable()) s->thread.join();
+    // Ask the lanes to drop their items and leave, then wait for the launch to end.
+    uint32_t one = 1;
+    cudaMemcpyAsync(&h->d_q->yield, &one, 4, cudaMemcpyHostToDevice, s->copy);
+    cudaStreamSynchronize(s->copy);
+    cudaStreamSynchronize(h->stream);
+    if (s->done_log) cudaFreeHost(s->done_log);
+    if (s->copy) cudaStreamDestroy(s->copy);
+    if (s->kernel_done) cudaEventDestroy(s->kernel_done);
+    h->server = nullptr;
+    delete s;
+    return CCS_OK;
+}
+
+}  // namespace ccs
+
+extern "C" int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* opts) {
+    if (!h || slots <= 0) return fail(CCS_E_ARG, "bad arguments");
+    if (!h->d_table) return fail(CCS_E_STATE, "no table loaded");
+    if (h->server) return fail(CCS_E_STATE, "server already running");
+    CCS_TRY(ensure_search_buffers(h, (uint32_t)slots));
+    auto s = std::make_unique<Server>();
+    s->h = h;
+    if (opts) s->opts = *opts;
+    s->n_slots = (uint32_t)slots;
+    CCS_CUDA_TRY(cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking));
+    CCS_CUDA_TRY(cudaEventCreateWithFlags(&s->kernel_done, cudaEventDisableTiming));
+    s->log_cap = 2u * (uint32_t)slots + 64u;
+    CCS_CUDA_TRY(cudaHostAlloc(&s->done_log, 8ull * s->log_cap, cudaHostAllocMapped));
+    std::memset(s->done_log, 0, 8ull * s->log_cap);
+    CCS_CUDA_TRY(cudaHostGetDevicePointer(&s->d_done_log, s->done_log, 0));
+    fill_params(h, opts, &s->P);
+    s->P.done_log = s->d_done_log;
+    s->P.done_log_cap = s->log_cap;
+    s->grid = grid_for(h, opts);
+    QueueState q;
+    std::memset(&q, 0, sizeof q);
+    CCS_CUDA_TRY(cudaMemsetAsync(h->d_ring, 0xFF, sizeof(unsigned long long) * (h->ring_cap + h->slot_cap), s->copy));
+    CCS_CUDA_TRY(cudaMemcpyAsync(h->d_q, &q, sizeof q, cudaMemcpyHostToDevice, s->copy));
+    CCS_CUDA_TRY(cudaStreamSynchronize(s->copy));
+    s->slot_request.assign(h->slot_cap, 0);
+    for (uint32_t i = (uint32_t)slots; i-- > 0;) s->free_slots.push_back(i);
+    Server* raw = s.release();
+    h->server = raw;
+    raw->thread = std::thread([raw] { raw->run(); });
+    return CCS_OK;
+}
+
+extern "C" int ccs_server_submit(ccs_handle* h, const uint32_t* state, uint64_t* request_id) {
+    if (!h || !state) return fail(CCS_E_ARG, "NULL argument");
+    Server* s = h->server;
+    if (!s) return fail(CCS_E_STATE, "server not running");
+    if (!is_legal(unpack(state))) return fail(CCS_E_ARG, "not a legal position");
+    std::array<uint32_t, 5> st;
+    std::memcpy(st.data(), state, 20);
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (s->stop) return fail(s->error ? s->error : CCS_E_STATE, "server stopped: %s", s->error_msg.c_str());
+        uint64_t id = s->next_id++;
+        s->pending.emplace_back(id, st);
+        if (request_id) *request_id = id;
+    }
+    s->cv.notify_all();
+    return CCS_OK;
+}
+
+extern "C" int ccs_server_poll(ccs_handle* h, int max_out, uint64_t* request_ids, ccs_result* results, int* n_out) {
+    if (!h || !n_out || (max_out > 0 && (!request_ids || !results))) return fail(CCS_E_ARG, "NULL argument");
+    Server* s = h->server;
+    if (!s) return fail(CCS_E_STATE, "server not running");
+    std::lock_guard<std::mutex> lock(s->mu);
+    int k = 0;
+    while (k < max_out && !s->finished.empty()) {
+        request_ids[k] = s->finished.front().first;
+        results[k] = s->finished.front().second;
+        s->finished.pop_front();
+        ++k;
+    }
+    *n_out = k;
+    if (k == 0 && s->error) return fail(s->error, "server stopped: %s", s->error_msg.c_str());
+    return CCS_OK;
+}
+
+extern "C" int ccs_server_stop(ccs_handle* h) {
+    if (!h) return fail(CCS_E_ARG, "NULL handle");
+    return server_stop(h);
+}

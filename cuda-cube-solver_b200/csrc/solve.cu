@@ -1,0 +1,179 @@
+// libccs: batched solving and the continuous-batching server.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstring>
+#include <vector>
+
+#include "ccs_internal.h"
+#include "dispatch.cuh"
+#include "search_kernel.cuh"
+
+using namespace ccs;
+
+namespace ccs {
+
+constexpr int SEARCH_THREADS = 256;
+
+int ensure_search_buffers(ccs_handle* h, uint32_t slots) {
+    CCS_CUDA_TRY(cudaSetDevice(h->device));
+    if (!h->d_prefix[0]) {
+        for (int L = 0; L <= MAX_PLEN; ++L) {
+            std::vector<uint32_t> p = canonical_prefixes(L);
+            h->n_prefix[L] = (uint32_t)p.size();
+            CCS_CUDA_TRY(cudaMalloc(&h->d_prefix[L], p.size() * 4));
+            CCS_CUDA_TRY(cudaMemcpy(h->d_prefix[L], p.data(), p.size() * 4, cudaMemcpyHostToDevice));
+        }
+    }
+    if (!h->d_q) CCS_CUDA_TRY(cudaMalloc(&h->d_q, sizeof(QueueState)));
+    if (slots > h->slot_cap) {
+        cudaFree(h->d_slots);
+        cudaFree(h->d_ring);
+        h->d_slots = nullptr;
+        h->d_ring = nullptr;
+        h->slot_cap = 0;
+        uint32_t cap = std::max<uint32_t>(slots, 64u);
+        CCS_CUDA_TRY(cudaMalloc(&h->d_slots, sizeof(Slot) * cap));
+        // ring: each slot has at most one queued iteration; admission ring: one entry per slot
+        CCS_CUDA_TRY(cudaMalloc(&h->d_ring, sizeof(unsigned long long) * (3ull * cap + 64)));
+        h->slot_cap = cap;
+        h->ring_cap = 2 * cap + 64;
+    }
+    return CCS_OK;
+}
+
+void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
+    std::memset(P, 0, sizeof *P);
+    P->slots = h->d_slots;
+    P->q = h->d_q;
+    P->ring = h->d_ring;
+    P->ring_cap = h->ring_cap;
+    P->admit = h->d_ring + h->ring_cap;
+    P->admit_cap = h->slot_cap;
+    P->n_slots = h->slot_cap;
+    P->classidx = h->d_classidx;
+    P->table = h->d_table;
+    for (int L = 0; L <= MAX_PLEN; ++L) {
+        P->prefixes[L] = h->d_prefix[L];
+        P->n_prefix[L] = h->n_prefix[L];
+    }
+    int base = o && o->base_plen > 0 ? o->base_plen : 4;
+    P->base_plen = (uint32_t)std::min(base, MAX_PLEN);
+    P->deeper_at[0] = (unsigned long long)(o && o->deeper_at0 > 0 ? o->deeper_at0 : 5e7);
+    P->deeper_at[1] = (unsigned long long)(o && o->deeper_at1 > 0 ? o->deeper_at1 : 3e9);
+    P->idle_limit = 1u << 21;  // ~8 s of idle polling (4 us back-off) before a warp leaves
+    P->done_log = nullptr;
+    P->done_log_cap = 0;
+}
+
+int grid_for(ccs_handle* h, const ccs_solve_opts* o) {
+    int bps = o && o->blocks_per_sm > 0 ? o->blocks_per_sm : 2;
+    return bps * h->sms;
+}
+
+int launch_kernel(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream) {
+    return dispatch_kind(h->kind, [&](auto M, auto N) {
+        return dispatch_fmt(h->format, [&](auto F) {
+            constexpr int MODE = decltype(M)::value, NEC = decltype(N)::value, FMT = decltype(F)::value;
+            search_kernel<MODE, NEC, FMT, SEARCH_THREADS><<<grid, SEARCH_THREADS, 0, stream>>>(h->d_tables, P);
+            CCS_CUDA_TRY(cudaGetLastError());
+            return CCS_OK;
+        });
+    });
+}
+
+// Host slot record for a new cube: frames, no iteration yet (the admitting lane computes the
+// root bounds and publishes the first one).
+void make_slot(const uint32_t state[5], uint32_t request, Slot* s) {
+    std::memset(s, 0, sizeof *s);
+    cube_frames(state, s->frame);
+    s->status = SLOT_ACTIVE;
+    s->ticket = TICKET_IDLE;
+    s->request = request;
+}
+
+void fill_result(const Slot& s, ccs_result* r) {
+    std::memset(r, 0, sizeof *r);
+    if (s.status == SLOT_SOLVED) {
+        r->status = CCS_OK;
+        r->length = (int32_t)s.sol_len;
+        std::memcpy(r->moves, s.sol, std::min<uint32_t>(s.sol_len, 24));
+    } else {
+        r->status = CCS_E_CHECK;
+        r->length = -1;
+    }
+    r->nodes = s.nodes;
+    r->probes = s.probes;
+    r->seconds = s.t_done > s.t_admit ? (double)(s.t_done - s.t_admit) * 1e-9 : 0.0;
+    for (int i = 0; i < 24; ++i) r->iter_nodes[i] = s.iter_nodes[i];
+}
+
+}  // namespace ccs
+
+extern "C" int ccs_solve(ccs_handle* h, const uint32_t* states, int n, const ccs_solve_opts* opts, ccs_result* results) {
+    if (!h || (n > 0 && (!states || !results))) return fail(CCS_E_ARG, "NULL argument");
+    if (!h->d_table) return fail(CCS_E_STATE, "no table loaded");
+    if (h->server) return fail(CCS_E_STATE, "the server owns this handle's search buffers");
+    if (n <= 0) return CCS_OK;
+    for (int i = 0; i < n; ++i)
+        if (!is_legal(unpack(states + 5ull * i))) return fail(CCS_E_ARG, "cube %d is not a legal position", i);
+    CCS_TRY(ensure_search_buffers(h, (uint32_t)n));
+    std::vector<Slot> host(n);
+    for (int i = 0; i < n; ++i) make_slot(states + 5ull * i, (uint32_t)i, &host[i]);
+    std::vector<unsigned long long> admit(n);
+    for (int i = 0; i < n; ++i) admit[i] = (unsigned long long)i;  // lap 0
+    QueueState q;
+    std::memset(&q, 0, sizeof q);
+    q.admit_tail = (unsigned long long)n;
+    SearchParams P;
+    fill_params(h, opts, &P);
+    cudaStream_t st = h->stream;
+    CCS_CUDA_TRY(cudaMemcpyAsync(h->d_slots, host.data(), sizeof(Slot) * n, cudaMemcpyHostToDevice, st));
+    CCS_CUDA_TRY(cudaMemsetAsync(h->d_ring, 0xFF, sizeof(unsigned long long) * (h->ring_cap + h->slot_cap), st));
+    CCS_CUDA_TRY(cudaMemcpyAsync(P.admit, admit.data(), 8ull * n, cudaMemcpyHostToDevice, st));
+    CCS_CUDA_TRY(cudaMemcpyAsync(h->d_q, &q, sizeof q, cudaMemcpyHostToDevice, st));
+
+    const int grid = grid_for(h, opts);
+    const double timeout = opts && opts->timeout_s > 0 ? opts->timeout_s : 0;
+    auto t0 = std::chrono::steady_clock::now();
+    double kernel_ms = 0;
+    int launches = 0;
+    unsigned long long prev_probes = ~0ull;
+    for (;;) {
+        CCS_CUDA_TRY(cudaEventRecord(h->ev0, st));
+        CCS_TRY(launch_kernel(h, P, grid, st));
+        CCS_CUDA_TRY(cudaEventRecord(h->ev1, st));
+        CCS_CUDA_TRY(cudaMemcpyAsync(&q, h->d_q, sizeof q, cudaMemcpyDeviceToHost, st));
+        CCS_CUDA_TRY(cudaStreamSynchronize(st));
+        float ms = 0;
+        CCS_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+        kernel_ms += ms;
+        ++launches;
+        if (q.active == 0 && q.admit_head >= q.admit_tail) break;
+        // A launch ends only when every warp is out of work; if a relaunch found none either,
+        // an iteration was lost.
+        if (q.probes == prev_probes)
+            return fail(CCS_E_CHECK, "search made no progress (%u cubes unfinished, error bits %u)", q.active, q.error);
+        prev_probes = q.probes;
+        double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (timeout > 0 && el > timeout)
+            return fail(CCS_E_TIMEOUT, "solve did not finish in %.1f s (%u cubes still searching)", timeout, q.active);
+        if (launches > 100000) return fail(CCS_E_TIMEOUT, "too many relaunches");
+    }
+    h->last_kernel_ms = kernel_ms;
+    h->last_probes = q.probes;
+    h->last_launches = launches;
+    CCS_CUDA_TRY(cudaMemcpyAsync(host.data(), h->d_slots, sizeof(Slot) * n, cudaMemcpyDeviceToHost, st));
+    CCS_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int i = 0; i < n; ++i) fill_result(host[i], &results[i]);
+    if (q.error & ERR_BOUND) return fail(CCS_E_CHECK, "a search passed the largest possible bound");
+    return CCS_OK;
+}
+
+extern "C" int ccs_last_solve_stats(ccs_handle* h, double* kernel_ms, uint64_t* probes, int* launches) {
+    if (!h) return fail(CCS_E_ARG, "NULL handle");
+    if (kernel_ms) *kernel_ms = h->last_kernel_ms;
+    if (probes) *probes = h->last_probes;
+    if (launches) *launches = h->last_launches;
+    return CCS_OK;
+}

@@ -1,0 +1,242 @@
+// libccs: building (BFS) and loading solving tables.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bfs_kernel.cuh"
+#include "ccs_internal.h"
+#include "dispatch.cuh"
+
+using namespace ccs;
+
+namespace {
+
+constexpr size_t CHUNK_BYTES = 256ull << 20;  // host staging for file I/O (the reference's 2^26 words)
+
+struct PinnedBuffer {
+    void* p = nullptr;
+    explicit PinnedBuffer(size_t n) {
+        if (cudaMallocHost(&p, n) != cudaSuccess) p = nullptr;
+    }
+    ~PinnedBuffer() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+void log_msg(ccs_log_fn log, const char* fmt, ...) {
+    if (!log) return;
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    log(buf);
+}
+
+int write_device_file(const void* dptr, uint64_t n_bytes, const std::string& path, cudaStream_t stream) {
+    PinnedBuffer buf(CHUNK_BYTES);
+    if (!buf.p) return fail(CCS_E_NOMEM, "pinned staging buffer");
+    std::string tmp = path + ".tmp";  // a crash mid-write must not leave a table that looks complete
+    FILE* f = fopen(tmp.c_str(), "wb");
+    if (!f) return fail(CCS_E_FILE, "%s: cannot open for writing", tmp.c_str());
+    for (uint64_t off = 0; off < n_bytes; off += CHUNK_BYTES) {
+        size_t n = (size_t)std::min<uint64_t>(CHUNK_BYTES, n_bytes - off);
+        cudaError_t e = cudaMemcpyAsync(buf.p, (const char*)dptr + off, n, cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) {
+            fclose(f);
+            return fail(CCS_E_CUDA, "copy to host: %s", cudaGetErrorString(e));
+        }
+        if (fwrite(buf.p, 1, n, f) != n) {
+            fclose(f);
+            return fail(CCS_E_FILE, "%s: write failed", tmp.c_str());
+        }
+    }
+    if (fclose(f) != 0) return fail(CCS_E_FILE, "%s: close failed", tmp.c_str());
+    if (std::rename(tmp.c_str(), path.c_str()) != 0) return fail(CCS_E_FILE, "rename %s -> %s failed", tmp.c_str(), path.c_str());
+    return CCS_OK;
+}
+
+}  // namespace
+
+extern "C" int ccs_load_table(ccs_handle* h, const char* kind, int format, const char* path) {
+    if (!h || !kind || !path) return fail(CCS_E_ARG, "NULL argument");
+    if (format != CCS_FMT_BLOCK && format != CCS_FMT_B3) return fail(CCS_E_ARG, "unknown table format %d", format);
+    CCS_TRY(set_kind(h, kind));
+    uint64_t want = table_bytes_for(h->kind, format);
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(CCS_E_FILE, "%s not found", path);
+    fseek(f, 0, SEEK_END);
+    long long size = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    if (size < 0 || (uint64_t)size != want) {
+        fclose(f);
+        return fail(CCS_E_FILE, "%s: size %lld, expected %llu", path, size, (unsigned long long)want);
+    }
+    CCS_CUDA_TRY(cudaSetDevice(h->device));
+    free_table(h);
+    uint32_t* d = nullptr;
+    if (cudaMalloc(&d, want) != cudaSuccess) {
+        fclose(f);
+        return fail(CCS_E_NOMEM, "device allocation of %llu bytes for the table", (unsigned long long)want);
+    }
+    PinnedBuffer buf(CHUNK_BYTES);
+    if (!buf.p) {
+        fclose(f);
+        cudaFree(d);
+        return fail(CCS_E_NOMEM, "pinned staging buffer");
+    }
+    for (uint64_t off = 0; off < want; off += CHUNK_BYTES) {
+        size_t n = (size_t)std::min<uint64_t>(CHUNK_BYTES, want - off);
+        if (fread(buf.p, 1, n, f) != n) {
+            fclose(f);
+            cudaFree(d);
+            return fail(CCS_E_FILE, "%s: short read", path);
+        }
+        cudaError_t e = cudaMemcpyAsync((char*)d + off, buf.p, n, cudaMemcpyHostToDevice, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) {
+            fclose(f);
+            cudaFree(d);
+            return fail(CCS_E_CUDA, "copy to device: %s", cudaGetErrorString(e));
+        }
+    }
+    fclose(f);
+    h->d_table = d;
+    h->table_bytes = want;
+    h->format = format;
+    return CCS_OK;
+}
+
+extern "C" int ccs_build_table(ccs_handle* h, const char* kind, int format, const char* out_path, int keep_resident,
+                               uint64_t* depth_counts, int max_depths, int* n_depths, double* seconds,
+                               ccs_log_fn log) {
+    if (!h || !kind) return fail(CCS_E_ARG, "NULL argument");
+    if (format != CCS_FMT_BLOCK && format != CCS_FMT_B3) return fail(CCS_E_ARG, "unknown table format %d", format);
+    CCS_TRY(set_kind(h, kind));
+    CCS_CUDA_TRY(cudaSetDevice(h->device));
+    const KindDesc k = h->kind;
+    const uint64_t n_entries = k.n_entries;
+    const uint64_t n_chunks = (n_entries + 15) / 16;
+    auto t0 = std::chrono::steady_clock::now();
+
+    if (keep_resident) free_table(h);  // make room; the new table replaces it
+    DeviceBuffer<uint8_t> depth(n_chunks * 16);
+    DeviceBuffer<unsigned long long> counter(40);
+    if (!depth.ok() || !counter.ok())
+        return fail(CCS_E_NOMEM, "device allocation for the BFS (%llu bytes)", (unsigned long long)(n_chunks * 16));
+    CCS_CUDA_TRY(cudaMemsetAsync(depth.p, 0xFF, n_chunks * 16, h->stream));
+    CCS_CUDA_TRY(cudaMemsetAsync(counter.p, 0, 40 * sizeof(unsigned long long), h->stream));
+
+    BfsParams P;
+    P.depth = depth.p;
+    P.n_entries = n_entries;
+    P.n_chunks = n_chunks;
+    P.classidx = h->d_classidx;
+    P.class_rep = h->d_class_rep;
+    P.class_stab = h->d_class_stab;
+    P.counter = counter.p;
+    const int grid = h->sms * 8;
+
+    std::vector<uint64_t> counts;
+    auto read_counter = [&](uint64_t* v) -> int {
+        CCS_CUDA_TRY(cudaMemcpyAsync(v, counter.p, 8, cudaMemcpyDeviceToHost, h->stream));
+        CCS_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        CCS_CUDA_TRY(cudaMemsetAsync(counter.p, 0, 8, h->stream));
+        return CCS_OK;
+    };
+    CCS_TRY(dispatch_kind(k, [&](auto M, auto N) {
+        constexpr int MODE = decltype(M)::value, NEC = decltype(N)::value;
+        bfs_seed<MODE, NEC><<<1, 32, 0, h->stream>>>(h->d_tables, P);
+        CCS_CUDA_TRY(cudaGetLastError());
+        uint64_t found = 0;
+        CCS_TRY(read_counter(&found));
+        counts.push_back(found);
+        uint64_t remaining = n_entries - found;
+        for (uint32_t d = 0; remaining; ++d) {
+            if (d >= 30) return fail(CCS_E_CHECK, "BFS deeper than 30");
+            // The reference's rule (table.py:112): forward while the frontier is under a
+            // quarter of the unvisited entries, backward afterwards.
+            bool forward = counts.back() < remaining / 4;
+            auto ts = std::chrono::steady_clock::now();
+            if (forward) bfs_forward<MODE, NEC><<<grid, 256, 0, h->stream>>>(h->d_tables, P, d);
+            else bfs_backward<MODE, NEC><<<grid, 256, 0, h->stream>>>(h->d_tables, P, d);
+            CCS_CUDA_TRY(cudaGetLastError());
+            CCS_TRY(read_counter(&found));
+            double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count();
+            log_msg(log, "depth %2u %s found %14llu (%7.2fs)", d + 1, forward ? "fwd" : "bwd", (unsigned long long)found, dt);
+            if (found == 0) return fail(CCS_E_UNREACHABLE, "%llu entries unreachable", (unsigned long long)remaining);
+            if (found > remaining) return fail(CCS_E_CHECK, "BFS found more entries than remain");
+            counts.push_back(found);
+            remaining -= found;
+        }
+        return CCS_OK;
+    }));
+
+    // Self-check: the histogram of depths equals the per-pass counts, nothing left unvisited.
+    {
+        DeviceBuffer<unsigned long long> hist(33);
+        if (!hist.ok()) return fail(CCS_E_NOMEM, "histogram buffer");
+        CCS_CUDA_TRY(cudaMemsetAsync(hist.p, 0, 33 * 8, h->stream));
+        bfs_histogram<<<h->sms * 4, 256, 0, h->stream>>>(depth.p, n_entries, hist.p);
+        CCS_CUDA_TRY(cudaGetLastError());
+        unsigned long long hh[33];
+        CCS_CUDA_TRY(cudaMemcpyAsync(hh, hist.p, sizeof hh, cudaMemcpyDeviceToHost, h->stream));
+        CCS_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        for (int i = 0; i < 33; ++i) {
+            uint64_t want = i < (int)counts.size() ? counts[i] : 0;
+            if (hh[i] != want)
+                return fail(CCS_E_CHECK, "histogram of depth %d is %llu, BFS counted %llu", i, hh[i], (unsigned long long)want);
+        }
+    }
+
+    // Encode the solving file.
+    const uint64_t n_blk = (n_entries + BLOCK_ENTRIES - 1) / BLOCK_ENTRIES;
+    uint32_t* d_blk = nullptr;
+    if (cudaMalloc(&d_blk, n_blk * 32) != cudaSuccess) return fail(CCS_E_NOMEM, "block table allocation");
+    encode_block<<<h->sms * 8, 256, 0, h->stream>>>(depth.p, n_entries, n_blk, d_blk);
+    cudaError_t e = cudaGetLastError();
+    uint32_t* d_out = d_blk;
+    uint64_t out_bytes = n_blk * 32;
+    if (e == cudaSuccess && format == CCS_FMT_B3) {
+        const uint64_t n_b3 = (n_entries + B3_ENTRIES - 1) / B3_ENTRIES;
+        uint32_t* d_b3 = nullptr;
+        if (cudaMalloc(&d_b3, n_b3 * 32) != cudaSuccess) {
+            cudaFree(d_blk);
+            return fail(CCS_E_NOMEM, "base-3 table allocation");
+        }
+        encode_b3<<<(unsigned)((n_b3 + 127) / 128), 128, 0, h->stream>>>(depth.p, d_blk, n_entries, n_b3, d_b3);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        cudaFree(d_blk);
+        d_out = d_b3;
+        out_bytes = n_b3 * 32;
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+        cudaFree(d_out);
+        return fail(CCS_E_CUDA, "encoding the table: %s", cudaGetErrorString(e));
+    }
+    double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (seconds) *seconds = secs;
+    if (n_depths) *n_depths = (int)counts.size();
+    if (depth_counts)
+        for (int i = 0; i < (int)counts.size() && i < max_depths; ++i) depth_counts[i] = counts[i];
+
+    int rc = CCS_OK;
+    if (out_path) rc = write_device_file(d_out, out_bytes, out_path, h->stream);
+    if (rc == CCS_OK && keep_resident) {
+        free_table(h);
+        h->d_table = d_out;
+        h->table_bytes = out_bytes;
+        h->format = format;
+    } else {
+        cudaFree(d_out);
+    }
+    return rc;
+}

@@ -1,0 +1,251 @@
+"""ctypes binding of libccs, the C-ABI library built for sm_100a (``include/ccs.h``).
+
+This is the only way the package reaches the GPU: there is no CPU or CuPy fallback.  If the
+library is missing, importing this module raises ``ImportError`` naming the build command.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(os.environ.get("CCS_LIB", Path(__file__).with_name("_lib") / "libccs.so"))
+
+CCS_OK = 0
+CCS_E_CUDA = -1
+CCS_E_NOMEM = -2
+CCS_E_ARG = -3
+CCS_E_FILE = -4
+CCS_E_CHECK = -5
+CCS_E_UNREACHABLE = -6
+CCS_E_STATE = -7
+CCS_E_TIMEOUT = -8
+FORMATS = {"block": 0, "b3": 1}
+
+
+class CcsError(RuntimeError):
+    """A libccs call failed; ``code`` is the CCS_E_* value."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+class SolveOpts(ctypes.Structure):
+    _fields_ = [
+        ("base_plen", ctypes.c_int),
+        ("deeper_at0", ctypes.c_double),
+        ("deeper_at1", ctypes.c_double),
+        ("blocks_per_sm", ctypes.c_int),
+        ("threads", ctypes.c_int),
+        ("timeout_s", ctypes.c_double),
+    ]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int32),
+        ("length", ctypes.c_int32),
+        ("moves", ctypes.c_uint8 * 24),
+        ("nodes", ctypes.c_uint64),
+        ("probes", ctypes.c_uint64),
+        ("seconds", ctypes.c_double),
+        ("iter_nodes", ctypes.c_uint64 * 24),
+    ]
+
+
+LOG_FN = ctypes.CFUNCTYPE(None, ctypes.c_char_p)
+
+# name -> (argtypes); every function returns int (status) except where noted.
+_P = ctypes.POINTER
+_SIGS = {
+    "ccs_version": [],
+    "ccs_mem_info": [ctypes.c_int, _P(ctypes.c_uint64), _P(ctypes.c_uint64)],
+    "ccs_device_sms": [ctypes.c_int, _P(ctypes.c_int)],
+    "ccs_open": [ctypes.c_int, _P(ctypes.c_void_p)],
+    "ccs_close": [ctypes.c_void_p],
+    "ccs_kind_info": [ctypes.c_char_p, _P(ctypes.c_int), _P(ctypes.c_uint64)],
+    "ccs_register_group_kind": [ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
+    "ccs_kind_tables": [ctypes.c_char_p] + [ctypes.c_void_p] * 5,
+    "ccs_set_kind": [ctypes.c_void_p, ctypes.c_char_p],
+    "ccs_load_table": [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p],
+    "ccs_build_table": [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
+                        ctypes.c_void_p, ctypes.c_int, _P(ctypes.c_int), _P(ctypes.c_double), LOG_FN],
+    "ccs_table_bytes": [ctypes.c_void_p, _P(ctypes.c_uint64)],
+    "ccs_table_copy": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64],
+    "ccs_index": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
+    "ccs_unrank": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p],
+    "ccs_lower_bound": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p],
+    "ccs_root_bounds": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p],
+    "ccs_solve": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _P(SolveOpts), ctypes.c_void_p],
+    "ccs_last_solve_stats": [ctypes.c_void_p, _P(ctypes.c_double), _P(ctypes.c_uint64), _P(ctypes.c_int)],
+    "ccs_server_start": [ctypes.c_void_p, ctypes.c_int, _P(SolveOpts)],
+    "ccs_server_submit": [ctypes.c_void_p, ctypes.c_void_p, _P(ctypes.c_uint64)],
+    "ccs_server_poll": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, _P(ctypes.c_int)],
+    "ccs_server_stop": [ctypes.c_void_p],
+}
+EXPORTED = tuple(_SIGS) + ("ccs_last_error",)
+
+
+def _load():
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
+                          f"or `make -C cuda-cube-solver_b200/csrc`")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    for name, args in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+    lib.ccs_last_error.argtypes = []
+    lib.ccs_last_error.restype = ctypes.c_char_p
+    return lib
+
+
+lib = _load()
+
+
+def check(rc: int) -> None:
+    if rc != CCS_OK:
+        raise CcsError(rc, lib.ccs_last_error().decode(errors="replace"))
+
+
+def _ptr(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def mem_info(device: int = 0) -> tuple[int, int]:
+    free, total = ctypes.c_uint64(), ctypes.c_uint64()
+    check(lib.ccs_mem_info(device, ctypes.byref(free), ctypes.byref(total)))
+    return free.value, total.value
+
+
+def kind_info(kind: str) -> tuple[int, int]:
+    nec, n = ctypes.c_int(), ctypes.c_uint64()
+    check(lib.ccs_kind_info(kind.encode(), ctypes.byref(nec), ctypes.byref(n)))
+    return nec.value, n.value
+
+
+def register_group_kind(name: str, gens) -> None:
+    perms = np.ascontiguousarray([g[0] for g in gens], dtype=np.int32).reshape(-1)
+    flips = np.ascontiguousarray([g[1] for g in gens], dtype=np.int32).reshape(-1)
+    check(lib.ccs_register_group_kind(name.encode(), len(gens), _ptr(perms), _ptr(flips)))
+
+
+def kind_tables(kind: str) -> dict[str, np.ndarray]:
+    out = {"classidx": np.zeros(153090, np.uint32), "class_rep": np.zeros(9930, np.uint32),
+           "class_stab": np.zeros(9930, np.uint16), "gen_class": np.zeros(384, np.uint16),
+           "gen_rep": np.zeros((2, 384), np.uint16)}
+    check(lib.ccs_kind_tables(kind.encode(), *(_ptr(out[k]) for k in
+                                               ("classidx", "class_rep", "class_stab", "gen_class", "gen_rep"))))
+    return out
+
+
+def solve_opts(base_plen: int = 4, deeper_at: tuple[float, float] = (5e7, 3e9), blocks_per_sm: int = 0,
+               threads: int = 0, timeout_s: float = 0.0) -> SolveOpts:
+    return SolveOpts(base_plen, float(deeper_at[0]), float(deeper_at[1]), blocks_per_sm, threads, timeout_s)
+
+
+class Handle:
+    """An open libccs handle on one device (not thread-safe; the server calls are)."""
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        check(lib.ccs_open(device, ctypes.byref(self._h)))
+        self.device = device
+
+    def close(self) -> None:
+        if self._h:
+            lib.ccs_close(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_kind(self, kind: str) -> None:
+        check(lib.ccs_set_kind(self._h, kind.encode()))
+
+    def load_table(self, kind: str, fmt: str, path) -> None:
+        check(lib.ccs_load_table(self._h, kind.encode(), FORMATS[fmt], str(path).encode()))
+
+    def build_table(self, kind: str, fmt: str, out_path=None, keep_resident: bool = False, log=None):
+        counts = np.zeros(64, np.uint64)
+        n = ctypes.c_int()
+        secs = ctypes.c_double()
+        cb = LOG_FN(lambda m: log(m.decode())) if log else LOG_FN()
+        check(lib.ccs_build_table(self._h, kind.encode(), FORMATS[fmt],
+                                  None if out_path is None else str(out_path).encode(), int(keep_resident),
+                                  _ptr(counts), 64, ctypes.byref(n), ctypes.byref(secs), cb))
+        return [int(c) for c in counts[:n.value]], secs.value
+
+    def table_bytes(self) -> int:
+        n = ctypes.c_uint64()
+        check(lib.ccs_table_bytes(self._h, ctypes.byref(n)))
+        return n.value
+
+    def table_copy(self) -> np.ndarray:
+        out = np.empty(self.table_bytes(), np.uint8)
+        check(lib.ccs_table_copy(self._h, _ptr(out), out.nbytes))
+        return out
+
+    def index(self, states: np.ndarray, move: int = -1) -> tuple[np.ndarray, np.ndarray]:
+        states = np.ascontiguousarray(states, dtype=np.uint32).reshape(-1, 5)
+        idx = np.zeros(len(states), np.uint64)
+        out = np.zeros_like(states)
+        check(lib.ccs_index(self._h, _ptr(states), len(states), move, _ptr(idx), _ptr(out)))
+        return idx, out
+
+    def unrank(self, idx: np.ndarray) -> np.ndarray:
+        idx = np.ascontiguousarray(idx, dtype=np.uint64).reshape(-1)
+        out = np.zeros((len(idx), 5), np.uint32)
+        check(lib.ccs_unrank(self._h, _ptr(idx), len(idx), _ptr(out)))
+        return out
+
+    def lower_bound(self, states: np.ndarray) -> np.ndarray:
+        states = np.ascontiguousarray(states, dtype=np.uint32).reshape(-1, 5)
+        out = np.zeros(len(states), np.uint32)
+        check(lib.ccs_lower_bound(self._h, _ptr(states), len(states), _ptr(out)))
+        return out
+
+    def root_bounds(self, states: np.ndarray) -> np.ndarray:
+        states = np.ascontiguousarray(states, dtype=np.uint32).reshape(-1, 5)
+        out = np.zeros((len(states), 6), np.uint32)
+        check(lib.ccs_root_bounds(self._h, _ptr(states), len(states), _ptr(out)))
+        return out
+
+    def solve(self, states: np.ndarray, opts: SolveOpts | None = None):
+        states = np.ascontiguousarray(states, dtype=np.uint32).reshape(-1, 5)
+        results = (Result * len(states))()
+        check(lib.ccs_solve(self._h, _ptr(states), len(states), ctypes.byref(opts or solve_opts()),
+                            ctypes.cast(results, ctypes.c_void_p)))
+        return list(results)
+
+    def last_solve_stats(self) -> tuple[float, int, int]:
+        ms, probes, launches = ctypes.c_double(), ctypes.c_uint64(), ctypes.c_int()
+        check(lib.ccs_last_solve_stats(self._h, ctypes.byref(ms), ctypes.byref(probes), ctypes.byref(launches)))
+        return ms.value, probes.value, launches.value
+
+    # server
+    def server_start(self, slots: int, opts: SolveOpts | None = None) -> None:
+        check(lib.ccs_server_start(self._h, slots, ctypes.byref(opts or solve_opts())))
+
+    def server_submit(self, state: np.ndarray) -> int:
+        state = np.ascontiguousarray(state, dtype=np.uint32).reshape(5)
+        rid = ctypes.c_uint64()
+        check(lib.ccs_server_submit(self._h, _ptr(state), ctypes.byref(rid)))
+        return rid.value
+
+    def server_poll(self, max_out: int = 256):
+        ids = np.zeros(max_out, np.uint64)
+        results = (Result * max_out)()
+        n = ctypes.c_int()
+        check(lib.ccs_server_poll(self._h, max_out, _ptr(ids), ctypes.cast(results, ctypes.c_void_p), ctypes.byref(n)))
+        return [(int(ids[i]), results[i]) for i in range(n.value)]
+
+    def server_stop(self) -> None:
+        check(lib.ccs_server_stop(self._h))

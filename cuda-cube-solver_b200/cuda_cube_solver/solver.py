@@ -1,0 +1,196 @@
+"""Optimal HTM solver: IDA* on the GPU with a resident pruning table (the reference's ``solver.py``).
+
+Same public surface as the reference (``solver.py:1-325``): ``open_solver``, ``GpuSolver`` with
+``solve`` and ``root_h``, ``Solution``, ``TableNotFound``, ``NoTableFits``, ``frames``,
+``canonical_prefixes``, ``allowed``, ``parse_moves``.  The search itself runs in libccs: one
+persistent launch takes every cube of a ``solve`` call through its IDA* bounds on the device
+(no host round trip per bound), and a host check verifies every returned solution.
+"""
+
+from __future__ import annotations
+
+import re
+import time
+from dataclasses import dataclass, field
+from functools import lru_cache
+from pathlib import Path
+
+import numpy as np
+
+from cuda_cube_solver import kinds, native
+from cuda_cube_solver.cubie import MOVE_NAMES_HTM, MOVES_HTM, CubieState, apply_moves
+from cuda_cube_solver.device import state_words
+from cuda_cube_solver.geometry import axis_rotation
+
+
+def allowed(last: int, move: int) -> bool:
+    """Canonical order: never the same face twice in a row, opposite faces only as U-D, R-L, F-B."""
+
+    if last < 0:
+        return True
+    lf, mf = last // 3, move // 3
+    return mf != lf and not (lf >= 3 and mf == lf - 3)
+
+
+@lru_cache(maxsize=None)
+def canonical_prefixes(length: int) -> np.ndarray:
+    """All canonical move sequences of ``length``, lexicographic (each sequence's children in move order)."""
+
+    seqs = [()]
+    for _ in range(length):
+        seqs = [s + (m,) for s in seqs for m in range(18) if allowed(s[-1] if s else -1, m)]
+    return np.array(seqs, dtype=np.uint8).reshape(len(seqs), length)
+
+
+def frames(state: CubieState) -> list[CubieState]:
+    """The three axis frames of ``state`` (turned so each axis becomes U-D) followed by their inverses."""
+
+    rot = axis_rotation()
+    once = rot.conjugate(state)
+    axes = [state, once, rot.conjugate(once)]
+    return axes + [f.inverse() for f in axes]
+
+
+@dataclass
+class Solution:
+    moves: list[int]
+    nodes: int
+    seconds: float
+    iteration_nodes: list[tuple[int, int]] = field(default_factory=list)  # (bound, nodes)
+    probes: int = 0
+
+    def text(self) -> str:
+        return " ".join(MOVE_NAMES_HTM[m] for m in self.moves)
+
+
+class TableNotFound(FileNotFoundError):
+    """A pruning table file is missing."""
+
+
+class NoTableFits(RuntimeError):
+    """No table preset fits in the GPU memory budget."""
+
+
+def _table_file(tables: Path, name: str) -> Path:
+    path = tables / name
+    if not path.exists():
+        m = re.fullmatch(r"prune-ud-(\d+|[a-z0-9]+)(?:-blk)?(-b3)?\.bin", name)
+        hint = f"; build it with `cuda-cube-solver build-table --table {m[1]}{m[2] or ''} --out {tables}`" if m else ""
+        raise TableNotFound(f"{path} not found{hint}")
+    return path
+
+
+def open_solver(tables: Path = Path("tables"), memory="auto", table: str | None = None, build: bool = True,
+                log=print) -> "GpuSolver":
+    """A solver with the fastest table preset that fits ``memory`` (GB, or "auto": the free device
+    memory), or the preset named ``table`` (see ``kinds.PRESETS``).  A missing table is built first
+    unless ``build`` is False."""
+
+    from cuda_cube_solver import table as tables_mod
+
+    tables = Path(tables)
+    if tables.suffix == ".bin":
+        tables = tables.parent
+    preset = kinds.pick(tables, memory, table)[0]
+    if preset is None:
+        raise NoTableFits("no table fits in that GPU memory (the smallest, 304, needs 1.8 GB)")
+    if not (tables / preset.file).exists():
+        if not build:
+            raise TableNotFound(f"{tables / preset.file} not found")
+        log(f"building table {preset.name} ({preset.table_bytes / 1e9:.2f} GB) in {tables}/")
+        log(f"wrote {tables_mod.build_preset(tables, preset, log=lambda m: log(f'  {m}'))}")
+    return GpuSolver(tables, kind=preset.kind, table_format=preset.format)
+
+
+class GpuSolver:
+    """IDA* solver over a solving table resident on the GPU.
+
+    ``prefix_len``: prefix length of the work items of a cube's first iterations; an iteration of
+    at least ``deeper_prefix_at[i]`` nodes makes the next one use one move more.  ``grid`` is the
+    number of blocks of the persistent launch (default 2 per SM); ``block`` is fixed at 256.
+    ``handle``: an already open ``native.Handle`` holding the table (``table_format`` and ``kind``
+    must then describe it), e.g. one that built it with ``keep_resident``.
+    """
+
+    def __init__(self, tables: Path = Path("tables"), prefix_len: int = 4, grid: int | None = None, block: int = 256,
+                 inverse: bool = True, collect_stats: bool = False, mode: str = "step", table_format: str = "block",
+                 kind="d4t", deeper_prefix_at: tuple[float, ...] = (5e7, 3e9), handle: native.Handle | None = None,
+                 device: int = 0):
+        if mode != "step" or not inverse:
+            raise ValueError("only the step search with inverse frames is built (mode='step', inverse=True)")
+        if block != 256:
+            raise ValueError("block must be 256")
+        tables = Path(tables)
+        if tables.suffix == ".bin":
+            tables = tables.parent
+        self.kind = kinds.get(kind) if isinstance(kind, str) else kind
+        self.table_format = table_format
+        if table_format not in native.FORMATS:
+            raise ValueError(f"unknown table format {table_format!r}")
+        self.prefix_len = prefix_len
+        self.deeper_prefix_at = tuple(deeper_prefix_at) + (float("inf"),) * (2 - len(deeper_prefix_at))
+        self.collect_stats = collect_stats
+        if handle is None:
+            handle = native.Handle(device)
+            fname = f"prune-ud-{self.kind.name}-{'b3' if table_format == 'b3' else 'blk'}.bin"
+            try:
+                handle.load_table(self.kind.name, table_format, _table_file(tables, fname))
+            except native.CcsError as exc:
+                raise ValueError(str(exc)) if exc.code == native.CCS_E_FILE else exc
+        self.handle = handle
+        sms = native.ctypes.c_int()
+        native.check(native.lib.ccs_device_sms(handle.device, native.ctypes.byref(sms)))
+        self.grid = grid or 2 * sms.value
+        self.block = block
+        self.last_kernel_ms = 0.0
+        self.last_probes = 0
+
+    @classmethod
+    def build_resident(cls, kind: str = "d4t", table_format: str = "block", log=None, device: int = 0, **kw):
+        """Build ``kind`` on the GPU and solve with it straight from device memory (no file)."""
+
+        h = native.Handle(device)
+        counts, secs = h.build_table(kind, table_format, None, keep_resident=True, log=log)
+        solver = cls(kind=kind, table_format=table_format, handle=h, **kw)
+        solver.build_counts, solver.build_seconds = counts, secs
+        return solver
+
+    def _opts(self, timeout_s: float = 0.0) -> native.SolveOpts:
+        sms = native.ctypes.c_int()
+        native.check(native.lib.ccs_device_sms(self.handle.device, native.ctypes.byref(sms)))
+        blocks_per_sm = max(1, round(self.grid / sms.value))
+        return native.solve_opts(self.prefix_len, self.deeper_prefix_at[:2], blocks_per_sm, 256, timeout_s)
+
+    def root_h(self, states: list[CubieState]) -> tuple[np.ndarray, np.ndarray]:
+        words = state_words(states)
+        frame_words = state_words([f for s in states for f in frames(s)]).reshape(len(states), 30)
+        return self.handle.root_bounds(words), frame_words
+
+    def solve(self, states: list[CubieState], log=None) -> list[Solution]:
+        if not states:
+            return []
+        words = state_words(states)
+        t0 = time.perf_counter()
+        results = self.handle.solve(words, self._opts())
+        self.last_kernel_ms, self.last_probes, _ = self.handle.last_solve_stats()
+        out = []
+        for state, r in zip(states, results):
+            if r.status != 0:
+                raise AssertionError(f"search failed with status {r.status}")
+            moves = list(r.moves[: r.length])
+            hist = [(b, int(r.iter_nodes[b])) for b in range(24) if r.iter_nodes[b]]
+            out.append(Solution(moves, int(r.nodes), float(r.seconds), hist, int(r.probes)))
+        if log:
+            log(f"{time.perf_counter() - t0:8.2f}s solved {len(out)}/{len(states)}")
+        for state, sol in zip(states, out):
+            if apply_moves(state, [MOVES_HTM[m] for m in sol.moves]) != CubieState():
+                raise AssertionError("solution does not solve the cube")
+        return out
+
+    def close(self) -> None:
+        self.handle.close()
+
+
+def parse_moves(text: str) -> list[int]:
+    index = {name: i for i, name in enumerate(MOVE_NAMES_HTM)}
+    return [index[tok] for tok in text.split()]

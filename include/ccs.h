@@ -1,0 +1,146 @@
+/* libccs: B200-native optimal 3x3 cube solving (half-turn metric) behind a C ABI.
+ *
+ * The library replaces the reference's kernel boundary: src/cuda_cube_solver/device.py:115-141
+ * (module(*defines) -> CuPy RawModule of kernels.cu, DeviceTables) and the kernel launches at
+ * solver.py:238-240,302 and table.py:72-79,103,115,118,136.  Host buffers are borrowed for the
+ * duration of a call; the library owns all device memory behind a handle.  Every call returns 0
+ * or a negative CCS_E_* code; ccs_last_error() gives the message of the last failure on the
+ * calling thread.  A handle is not reentrant: use one handle per host thread (the server entry
+ * points are the exception, see below).
+ *
+ * Packed state: 5 little-endian uint32 words, corner bytes cp | co << 3 (positions 0..7), edge
+ * bytes ep | eo << 4 (positions 0..11) -- the reference's device.pack_states (device.py:144-148).
+ * Moves are numbered 0..17 = U U2 U' R R2 R' F F2 F' D D2 D' L L2 L' B B2 B' (cubie.py:115-124).
+ */
+#ifndef CCS_H
+#define CCS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CCS_OK 0
+#define CCS_E_CUDA (-1)       /* a CUDA call failed */
+#define CCS_E_NOMEM (-2)      /* device or host allocation failed */
+#define CCS_E_ARG (-3)        /* bad argument: unknown kind / format, bad size (ValueError) */
+#define CCS_E_FILE (-4)       /* table file missing, unreadable or of the wrong size */
+#define CCS_E_CHECK (-5)      /* a self-check failed (AssertionError in the reference) */
+#define CCS_E_UNREACHABLE (-6)/* BFS found entries unreachable (RuntimeError in the reference) */
+#define CCS_E_STATE (-7)      /* call not valid in this state (no table loaded, server stopped) */
+#define CCS_E_TIMEOUT (-8)    /* a bounded wait ran out */
+
+#define CCS_FMT_BLOCK 0       /* 2-bit block table, "prune-ud-<kind>-blk.bin" */
+#define CCS_FMT_B3 1          /* base-3 block table, "prune-ud-<kind>-b3.bin" */
+
+typedef struct ccs_handle ccs_handle;
+
+typedef void (*ccs_log_fn)(const char* message);
+
+/* Library version, (major << 16) | minor. */
+int ccs_version(void);
+
+/* Message of the last failure on this thread ("" if none). */
+const char* ccs_last_error(void);
+
+/* Free and total memory of a device (kinds.pick, kinds.py:198-211, reads cudaMemGetInfo). */
+int ccs_mem_info(int device, uint64_t* free_bytes, uint64_t* total_bytes);
+
+/* Number of SMs of a device. */
+int ccs_device_sms(int device, int* sms);
+
+/* Open / close a handle on a device (replaces DeviceTables construction, device.py:125-141). */
+int ccs_open(int device, ccs_handle** out);
+int ccs_close(ccs_handle* h);
+
+/* Table kind by name: "304" or a group kind "s4", "d4f", "a4t", "d4t", "d4", "a4"
+ * (kinds.get, kinds.py:100-105).  Writes the E-content class count and the number of entries. */
+int ccs_kind_info(const char* kind, int* nec, uint64_t* n_entries);
+
+/* A custom group kind from generators (kinds.GroupKind, kinds.py:56-96): n_gens pairs of
+ * perm[4] and flips[4].  Registers it under `name` for the other calls.  Returns CCS_E_ARG with
+ * "<name>: group not normalised by the UD symmetries; ..." when symmetry reduction would be wrong. */
+int ccs_register_group_kind(const char* name, int n_gens, const int32_t* perms, const int32_t* flips);
+
+/* Constant tables of a kind (for cross-checks): corner classidx[153090], class_rep[9930],
+ * class_stab[9930], gen_class[384], gen_rep[2*384]; any pointer may be NULL. */
+int ccs_kind_tables(const char* kind, uint32_t* classidx, uint32_t* class_rep, uint16_t* class_stab,
+                    uint16_t* gen_class, uint16_t* gen_rep);
+
+/* Select the table kind used by ccs_index / ccs_unrank without loading a table. */
+int ccs_set_kind(ccs_handle* h, const char* kind);
+
+/* Load a solving table file into device memory (table.load_device, table.py:28-38; size checked
+ * against the kind and format like table.py:36-37).  Replaces any table already loaded. */
+int ccs_load_table(ccs_handle* h, const char* kind, int format, const char* path);
+
+/* Build a table on the device (table.generate + build_preset, table.py:82-129,170-200): exact
+ * BFS, histogram self-check, encode in `format`.  If out_path is not NULL the solving file is
+ * written there (through "<out_path>.tmp" and a rename).  If keep_resident, the solving table
+ * stays loaded in the handle as if ccs_load_table had been called.  depth_counts receives up to
+ * max_depths per-depth entry counts, n_depths their number; seconds the build time (GPU work,
+ * without the file write).  log may be NULL. */
+int ccs_build_table(ccs_handle* h, const char* kind, int format, const char* out_path, int keep_resident,
+                    uint64_t* depth_counts, int max_depths, int* n_depths, double* seconds, ccs_log_fn log);
+
+/* Copy the loaded solving table (n_bytes = its size) to host memory. */
+int ccs_table_bytes(ccs_handle* h, uint64_t* n_bytes);
+int ccs_table_copy(ccs_handle* h, void* dst, uint64_t n_bytes);
+
+/* Index of packed states under the loaded kind (the reference's probe_index kernel,
+ * kernels.cu:626-642): move >= 0 right-multiplies by that move first, move <= -2 left-multiplies
+ * by move -2 - move, -1 leaves the state.  out_idx[n], out_states[n*5] (may be NULL). */
+int ccs_index(ccs_handle* h, const uint32_t* states, int n, int move, uint64_t* out_idx, uint32_t* out_states);
+
+/* Representative state of each index (the reference's unrank, kernels.cu:294-379). */
+int ccs_unrank(ccs_handle* h, const uint64_t* idx, int n, uint32_t* out_states);
+
+/* Table lower bound of packed states (probe_block, kernels.cu:737-746). */
+int ccs_lower_bound(ccs_handle* h, const uint32_t* states, int n, uint32_t* out);
+
+/* Root bounds of cubes: the six frames' lower bounds (GpuSolver.root_h, solver.py:226-252). */
+int ccs_root_bounds(ccs_handle* h, const uint32_t* states, int n, uint32_t* out_h6);
+
+typedef struct ccs_solve_opts {
+    int base_plen;            /* prefix length of a cube's first iterations (reference: 4) */
+    double deeper_at0;        /* an iteration of >= this many nodes makes the next one use a */
+    double deeper_at1;        /*   prefix one move longer (reference: 5e7, 3e9)             */
+    int blocks_per_sm;        /* persistent grid = blocks_per_sm * SMs (0: default)         */
+    int threads;              /* threads per block: 128, 256 or 512 (0: default)            */
+    double timeout_s;         /* give up after this long (0: no limit)                      */
+} ccs_solve_opts;
+
+typedef struct ccs_result {
+    int32_t status;           /* 0 solved, < 0 error */
+    int32_t length;           /* optimal length in half-turn moves */
+    uint8_t moves[24];        /* the solution, `length` moves */
+    uint64_t nodes;           /* children generated over all iterations */
+    uint64_t probes;          /* table lookups */
+    double seconds;           /* admission to solution, device clock */
+    uint64_t iter_nodes[24];  /* nodes per IDA* bound (Solution.iteration_nodes) */
+} ccs_result;
+
+/* Solve n cubes together (GpuSolver.solve, solver.py:254-320): one persistent launch advances
+ * every cube through its IDA* bounds on the device.  results[n]. */
+int ccs_solve(ccs_handle* h, const uint32_t* states, int n, const ccs_solve_opts* opts, ccs_result* results);
+
+/* Device time of the last ccs_solve's search kernels (ms) and its total table probes. */
+int ccs_last_solve_stats(ccs_handle* h, double* kernel_ms, uint64_t* probes, int* launches);
+
+/* ---- server: continuous batching (thread-safe against each other) -------------------------
+ * ccs_server_start runs a service thread that owns a persistent search launch over `slots`
+ * cube slots; ccs_server_submit queues a cube (returns a request id), ccs_server_poll returns
+ * up to max_out finished results with their request ids.  Cubes that arrive while others are on
+ * the GPU are admitted into free slots without waiting for the running ones. */
+int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* opts);
+int ccs_server_submit(ccs_handle* h, const uint32_t* state, uint64_t* request_id);
+int ccs_server_poll(ccs_handle* h, int max_out, uint64_t* request_ids, ccs_result* results, int* n_out);
+int ccs_server_stop(ccs_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CCS_H */
