@@ -1,0 +1,304 @@
+"""Benchmark: optimal solves/s of uniformly random cubes on the d4t table, batched, on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl reference]
+
+One step = one batched solve (libccs persistent launch) of B uniformly random cubes (seeded)
+against the d4t table resident in HBM.  The table is built on the GPU first (untimed, its build
+time is reported).  ``value`` = cubes / device time of the search launches (CUDA events on the
+library's stream), max over ranks; ``e2e`` = the same through the public API
+(``GpuSolver.solve`` with host CubieState lists: packing, host->device copy, search,
+device->host copy of the results, host verification of every solution).  ``plain`` = one cube
+per call (the drop-in path), with p50 / p99 per-cube latency.  Under torchrun each rank is an
+independent replica on its own GPU with its own cubes (weak scaling, no collective on the data
+path; NCCL only for the barrier and the max-over-ranks timing).
+
+``--impl reference``: the reference's method on the host's CPU cores -- the CPU oracle's IDA*
+(oracle/ccs_oracle.c, a restatement of the reference's search) over the same cubes and table,
+rank 0 only, bounded to a short sample.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "cuda-cube-solver_b200"))
+
+METRIC = "optimal solves/s (uniform random cubes, d4t) batched vs plain; p50/p99 latency"
+SECTOR = 32  # bytes of one table probe (one 32-byte DRAM sector)
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {"hbm_gbs": 6650.0, "fallback": True}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples taken while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int, local: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    dev = torch.device("cuda", local) if torch.cuda.is_available() else torch.device("cpu")
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def shard(n_total: int, world: int, rank: int) -> slice:
+    """Replicas: rank r takes cubes [r * n, (r + 1) * n) of the seeded stream."""
+
+    return slice(rank * n_total, (rank + 1) * n_total)
+
+
+def cpu_arm(args, states, frames_words, table: np.ndarray, probes_per_cube: float | None) -> dict:
+    """The reference's method on host cores: the CPU oracle's IDA* over the cubes, all threads,
+    bounded by ``args.cpu_budget`` seconds.  Throughput counts finished cubes plus the unfinished
+    ones' work in cube units (their probes / mean probes of a cube)."""
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from oracle import Oracle
+
+    o = Oracle()
+    o.set_kind(args.kind)
+    threads = os.cpu_count() or 1
+    n = min(len(frames_words), max(threads * 2, 8))
+    t0 = time.perf_counter()
+    lengths, _, _, probes = o.solve_many(table, args.format, frames_words[:n], threads=threads,
+                                        budget_s=args.cpu_budget)
+    dt = time.perf_counter() - t0
+    done = lengths >= 0
+    per_cube = probes_per_cube or (float(probes[done].mean()) if done.any() else None)
+    units = float(done.sum()) + (float(probes[~done].sum()) / per_cube if per_cube else 0.0)
+    return {"value": units / dt, "unit": "cubes/s", "cores": threads, "kind": "port",
+            "sample": f"first {n} cubes of the workload, CPU oracle IDA* (oracle/ccs_oracle.c) on {threads} threads for "
+                      f"{dt:.1f} s: {int(done.sum())} solved, unfinished work counted at "
+                      f"{per_cube / 1e6 if per_cube else 0:.1f} M probes per cube",
+            "probes_per_s": float(probes.sum()) / dt}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=1024, help="cubes per step and rank")
+    ap.add_argument("--kind", default="d4t")
+    ap.add_argument("--format", default="block", choices=["block", "b3"])
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
+    ap.add_argument("--plain", type=int, default=32, help="cubes solved one per call for the plain numbers")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    args = ap.parse_args()
+
+    world, rank, local = dist_setup()
+    from cuda_cube_solver import native, workloads
+    from cuda_cube_solver.device import state_words
+    from cuda_cube_solver.solver import GpuSolver, frames
+
+    n_steps_cubes = args.batch * (args.warmup + args.steps)
+    all_states = workloads.uniform_cubes(n_steps_cubes * world, seed=args.seed)
+    my_states = all_states[shard(n_steps_cubes, world, rank)]
+    config = {"workload": f"uniform random cubes (seed {args.seed}), {args.kind} {args.format} table resident in HBM, "
+                          f"{args.batch} cubes per step per GPU",
+              "table": args.kind if args.format == "block" else f"{args.kind}-b3", "batch": args.batch,
+              "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (7.8 GB table, random probes)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        h = native.Handle(local)
+        h.build_table(args.kind, args.format, None, keep_resident=True)
+        table = h.table_copy()
+        h.close()
+        fr = np.stack([state_words(frames(s)).reshape(30) for s in my_states[: 4 * (os.cpu_count() or 1)]])
+        cpu = cpu_arm(args, my_states, fr, table, None)
+        out = {"metric": METRIC, "value": cpu["value"], "unit": "cubes/s", "n_gpus": 1, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": 1000.0 * args.batch / cpu["value"] if cpu["value"] else None,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/u32 integer",
+               "data": "synthetic", "config": config, "impl": "reference",
+               "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+               "e2e": {"value": cpu["value"], "unit": "cubes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(out))
+        return
+
+    # ---- setup (untimed): build the table on this GPU, keep it resident ----
+    t = time.perf_counter()
+    solver = GpuSolver.build_resident(args.kind, args.format, device=local)
+    build_s = time.perf_counter() - t
+    h = solver.handle
+    opts = solver._opts()
+    batches = [state_words(my_states[i * args.batch:(i + 1) * args.batch]) for i in range(args.warmup + args.steps)]
+
+    for i in range(args.warmup):
+        h.solve(batches[i], opts)
+
+    # ---- timed: K batched steps, device time of the search launches ----
+    barrier(world)
+    kernel_ms, probes, launches, wall = [], [], [], []
+    with ClockSampler(local) as clocks:
+        t_all = time.perf_counter()
+        for i in range(args.warmup, args.warmup + args.steps):
+            t0 = time.perf_counter()
+            res = h.solve(batches[i], opts)
+            wall.append(time.perf_counter() - t0)
+            ms, pr, ln = h.last_solve_stats()
+            kernel_ms.append(ms)
+            probes.append(pr)
+            launches.append(ln)
+            assert all(r.status == 0 for r in res)
+        t_all = time.perf_counter() - t_all
+    barrier(world)
+    dev_s = max_over_ranks(sum(kernel_ms) / 1000.0, world, local)
+    value = world * args.batch * args.steps / dev_s
+
+    # ---- e2e through the public API: host cubes in, verified Solutions out ----
+    barrier(world)
+    t0 = time.perf_counter()
+    for i in range(args.warmup, args.warmup + args.steps):
+        sols = solver.solve(my_states[i * args.batch:(i + 1) * args.batch])
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, local)
+    e2e = world * args.batch * args.steps / e2e_s
+
+    if rank != 0:
+        barrier(world)
+        return
+
+    # ---- plain: one cube per call (the drop-in path), per-cube latency ----
+    plain_lat = []
+    for s in my_states[: args.plain]:
+        t0 = time.perf_counter()
+        solver.solve([s])
+        plain_lat.append(time.perf_counter() - t0)
+    plain = {"cubes": len(plain_lat), "cubes_per_s": len(plain_lat) / sum(plain_lat),
+             "p50_s": float(np.percentile(plain_lat, 50)), "p99_s": float(np.percentile(plain_lat, 99)),
+             "worst_s": max(plain_lat)}
+
+    peaks = measured_peaks()
+    total_probes = sum(probes)
+    achieved = total_probes * SECTOR / (sum(kernel_ms) / 1000.0) / 1e9
+    peak = float(peaks["hbm_gbs"])
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "probes_per_s": total_probes / (sum(kernel_ms) / 1000.0),
+                "probes_per_cube": total_probes / (args.batch * args.steps),
+                "peak_source": "measured" if not peaks.get("fallback") else "fallback",
+                "note": "algorithmic bytes = 32-byte sector per table probe, counted on the device"}
+    traffic_file = ROOT / "profiles" / "search_traffic.json"
+    if traffic_file.exists():
+        tr = json.loads(traffic_file.read_text())
+        roofline["traffic"] = tr["dram_bytes_per_probe"] * total_probes / max(1, sum(launches))
+
+    cpu = None
+    if not args.no_cpu:
+        table = h.table_copy()
+        fr = np.stack([state_words(frames(s)).reshape(30) for s in my_states[: 4 * (os.cpu_count() or 1)]])
+        cpu = cpu_arm(args, my_states, fr, table, roofline["probes_per_cube"])
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    out = {"metric": METRIC, "value": value, "unit": "cubes/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1000.0 * dev_s / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "u8/u32 integer", "data": "synthetic",
+           "config": config,
+           "e2e": {"value": e2e, "unit": "cubes/s", "h2d_bytes_per_step": 20 * args.batch,
+                   "d2h_bytes_per_step": native.ctypes.sizeof(native.Result) * args.batch},
+           "gpu_launches": int(sum(launches)),
+           "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
+           "plain": plain, "table_build_s": build_s, "table_build_gpu_s": solver.build_seconds,
+           "wall_s_per_step": statistics.mean(wall)}
+    print(json.dumps(out))
+    barrier(world)
+
+
+if __name__ == "__main__":
+    main()

@@ -17,7 +17,7 @@ from pathlib import Path
 
 import numpy as np
 
-from cuda_cube_solver import kinds, native
+from cuda_cube_solver import coords, kinds, native
 from cuda_cube_solver.cubie import MOVE_NAMES_HTM, MOVES_HTM, CubieState, apply_moves
 from cuda_cube_solver.device import state_words
 from cuda_cube_solver.geometry import axis_rotation
@@ -182,13 +182,28 @@ class GpuSolver:
             out.append(Solution(moves, int(r.nodes), float(r.seconds), hist, int(r.probes)))
         if log:
             log(f"{time.perf_counter() - t0:8.2f}s solved {len(out)}/{len(states)}")
-        for state, sol in zip(states, out):
-            if apply_moves(state, [MOVES_HTM[m] for m in sol.moves]) != CubieState():
-                raise AssertionError("solution does not solve the cube")
+        if not verify_solutions(words, [sol.moves for sol in out]):
+            raise AssertionError("solution does not solve the cube")
         return out
 
     def close(self) -> None:
         self.handle.close()
+
+
+def verify_solutions(words: np.ndarray, solutions: list[list[int]]) -> bool:
+    """True if every move list takes its packed state (n, 5) to solved (the reference's host
+    self-check, solver.py:317-319, vectorised over cubes)."""
+
+    b = np.ascontiguousarray(words, np.uint32).reshape(-1, 5).view(np.uint8).reshape(-1, 20)
+    corners, edges = b[:, :8].copy(), b[:, 8:].copy()
+    longest = max((len(m) for m in solutions), default=0)
+    for j in range(longest):
+        col = np.array([m[j] if j < len(m) else -1 for m in solutions])
+        for mv in np.unique(col[col >= 0]):
+            rows = col == mv
+            corners[rows], edges[rows] = coords.apply_move(corners[rows], edges[rows], int(mv))
+    solved = np.concatenate([np.arange(8, dtype=np.uint8)[None], np.arange(12, dtype=np.uint8)[None]], axis=1)
+    return bool((np.concatenate([corners, edges], axis=1) == solved).all())
 
 
 def parse_moves(text: str) -> list[int]:

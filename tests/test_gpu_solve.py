@@ -1,0 +1,96 @@
+"""GPU solving: every solution solves its cube and its length is optimal -- equal to the CPU
+oracle's exhaustive IDA* on small scrambles and to the reference's reported optimal lengths on
+its random, distance-20 and superflip positions."""
+
+from __future__ import annotations
+
+import random
+
+import numpy as np
+import pytest
+
+from conftest import resident_handle
+from cuda_cube_solver import native
+from cuda_cube_solver.cubie import MOVES_HTM, CubieState, apply_moves
+from cuda_cube_solver.device import state_words
+from cuda_cube_solver.solver import GpuSolver, frames, parse_moves
+
+pytestmark = pytest.mark.gpu
+
+
+def small_scrambles(n=200, seed=0):
+    """Seeded 8-12 move HTM scrambles, no two consecutive turns of the same face."""
+
+    rng = random.Random(seed)
+    out = []
+    for _ in range(n):
+        length, seq = rng.randint(8, 12), []
+        while len(seq) < length:
+            m = rng.randrange(18)
+            if seq and m // 3 == seq[-1] // 3:
+                continue
+            seq.append(m)
+        out.append(seq)
+    return out
+
+
+def _state(moves):
+    return apply_moves(CubieState(), [MOVES_HTM[m] for m in moves])
+
+
+def _check_solutions(states, results):
+    for s, r in zip(states, results):
+        assert r.status == 0
+        assert apply_moves(s, [MOVES_HTM[m] for m in r.moves[: r.length]]) == CubieState()
+
+
+def test_small_scrambles_on_304_match_oracle(oracle):
+    h = resident_handle("304")
+    scr = small_scrambles()
+    states = [_state(s) for s in scr]
+    res = h.solve(state_words(states), native.solve_opts(timeout_s=300))
+    _check_solutions(states, res)
+    assert all(r.length <= len(s) for r, s in zip(res, scr))
+    oracle.set_kind("304")
+    table = h.table_copy()
+    fr = np.stack([state_words(frames(s)).reshape(30) for s in states[:80]])
+    lengths, _, _, _ = oracle.solve_many(table, "block", fr)
+    assert [r.length for r in res[:80]] == lengths.tolist()
+
+
+def test_random_cubes_match_reference_lengths(lengths_golden):
+    h = resident_handle("d4t")
+    cubes = lengths_golden["random1000"]
+    states = [_state(parse_moves(c["scramble"])) for c in cubes]
+    res = h.solve(state_words(states), native.solve_opts(timeout_s=600))
+    _check_solutions(states, res)
+    assert [r.length for r in res] == [c["length"] for c in cubes]
+    _, probes, _ = h.last_solve_stats()
+    assert probes == sum(r.probes for r in res)
+
+
+def test_distance20_and_hard_positions(lengths_golden):
+    h = resident_handle("d4")
+    cubes = lengths_golden["distance20"] + [lengths_golden["superflip"], lengths_golden["hard19"]]
+    states = [_state(parse_moves(c["scramble"])) for c in cubes]
+    res = h.solve(state_words(states), native.solve_opts(timeout_s=900))
+    _check_solutions(states, res)
+    assert [r.length for r in res] == [c["length"] for c in cubes]
+
+
+def test_solved_cube_and_public_api(lengths_golden):
+    h = resident_handle("d4t")
+    solver = GpuSolver(kind="d4t", handle=h)
+    sols = solver.solve([CubieState(), _state(parse_moves(lengths_golden["random1000"][1]["scramble"]))])
+    assert sols[0].moves == [] and sols[0].nodes == 0
+    assert len(sols[1].moves) == lengths_golden["random1000"][1]["length"]
+    assert sols[1].iteration_nodes and sols[1].iteration_nodes[-1][0] == len(sols[1].moves)
+    h6, words = solver.root_h([CubieState()])
+    assert h6.tolist() == [[0] * 6] and words.shape == (1, 30)
+
+
+def test_illegal_state_is_rejected():
+    h = resident_handle("304")
+    bad = state_words([CubieState(ep=(1, 0) + tuple(range(2, 12)))])
+    with pytest.raises(native.CcsError, match="not a legal position"):
+        h.solve(bad)

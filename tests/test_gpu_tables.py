@@ -1,0 +1,75 @@
+"""GPU table builds: per-depth counts equal the reference's known answers, the histogram
+self-check holds, and the files are byte-identical to the CPU oracle's independent build
+(tests/golden/table_sha256.json) -- the reference's table format, bit for bit."""
+
+from __future__ import annotations
+
+import hashlib
+import json
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, resident_handle
+from cuda_cube_solver import kinds, native
+
+pytestmark = pytest.mark.gpu
+
+
+def _sha(a: np.ndarray) -> str:
+    return hashlib.sha256(a.tobytes()).hexdigest()
+
+
+def _sha_golden():
+    p = GOLDEN / "table_sha256.json"
+    return json.loads(p.read_text()) if p.exists() else {}
+
+
+def test_304_counts_and_bytes(depth_golden):
+    h = resident_handle("304")
+    assert h.build_counts == depth_golden["304"]["depth_counts"]
+    assert h.table_bytes() == kinds.PRESET_BY_NAME["304"].table_bytes
+    ref = _sha_golden().get("304")
+    if ref:
+        assert _sha(h.table_copy()) == ref["block_sha256"]
+
+
+@pytest.mark.parametrize("name", ["d4t", "d4"])
+def test_big_group_tables_counts(depth_golden, name):
+    h = resident_handle(name)
+    assert h.build_counts == depth_golden[name]["depth_counts"]
+    assert sum(h.build_counts) == depth_golden[name]["entries"]
+    assert h.table_bytes() == kinds.PRESET_BY_NAME[name].table_bytes
+
+
+def test_s4_b3_counts_and_bytes(depth_golden):
+    h = native.Handle()
+    try:
+        counts, _ = h.build_table("s4", "b3", None, keep_resident=True)
+        assert counts == depth_golden["s4"]["depth_counts"]
+        assert h.table_bytes() == kinds.PRESET_BY_NAME["s4-b3"].table_bytes
+        ref = _sha_golden().get("s4")
+        if ref:
+            assert _sha(h.table_copy()) == ref["b3_sha256"]
+    finally:
+        h.close()
+
+
+def test_file_roundtrip_and_size_check(tmp_path):
+    h = resident_handle("304")
+    path = tmp_path / "prune-ud-304-blk.bin"
+    table = h.table_copy()
+    table.tofile(path)
+    h2 = native.Handle()
+    try:
+        h2.load_table("304", "block", path)
+        words = np.array([[0x03020100, 0x07060504, 0x03020100, 0x07060504, 0x0B0A0908]], np.uint32)
+        assert h2.lower_bound(words).tolist() == [0]
+        bad = tmp_path / "short.bin"
+        table[:1000].tofile(bad)
+        with pytest.raises(native.CcsError, match="size 1000"):
+            h2.load_table("304", "block", bad)
+        with pytest.raises(native.CcsError, match="not found"):
+            h2.load_table("304", "block", tmp_path / "missing.bin")
+    finally:
+        h2.close()
