@@ -261,9 +261,11 @@ def main() -> None:
         t0 = time.perf_counter()
         solver.solve([s])
         plain_lat.append(time.perf_counter() - t0)
-    plain = {"cubes": len(plain_lat), "cubes_per_s": len(plain_lat) / sum(plain_lat),
-             "p50_s": float(np.percentile(plain_lat, 50)), "p99_s": float(np.percentile(plain_lat, 99)),
-             "worst_s": max(plain_lat)}
+    plain = None
+    if plain_lat:
+        plain = {"cubes": len(plain_lat), "cubes_per_s": len(plain_lat) / sum(plain_lat),
+                 "p50_s": float(np.percentile(plain_lat, 50)), "p99_s": float(np.percentile(plain_lat, 99)),
+                 "worst_s": max(plain_lat)}
 
     peaks = measured_peaks()
     total_probes = sum(probes)

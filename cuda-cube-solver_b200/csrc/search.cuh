@@ -8,6 +8,7 @@ namespace ccs {
 constexpr uint32_t SLOT_FREE = 0, SLOT_ACTIVE = 1, SLOT_SOLVED = 2, SLOT_ERROR = 3;
 constexpr unsigned long long TICKET_IDLE = 0x7FFFFFFFull;  // ticket of a slot with no iteration: exhausted
 constexpr int MAX_PLEN = 6;
+constexpr uint32_t RING_RETIRED = 0xFFFFFFFFu;  // ring entry whose iteration is fully handed out
 constexpr uint32_t MAX_BOUND = 22;   // every position is solvable in 20 half-turn moves
 
 // One cube under search.  The ticket is the work counter of the current IDA* iteration
@@ -58,6 +59,7 @@ struct SearchParams {
     uint32_t base_plen;              // prefix length of a cube's first iterations
     unsigned long long deeper_at[2]; // an iteration of at least this many nodes -> one move longer
     uint32_t idle_limit;             // idle polls before a warp leaves (kernel relaunched by the host)
+    uint32_t spread;                 // lanes take items from up to this many queued iterations
     unsigned long long* done_log;    // host-mapped completion log (server), may be null
     uint32_t done_log_cap;
 };

@@ -132,8 +132,8 @@ enum FetchResult { FETCH_OK = 0, FETCH_EMPTY = 1, FETCH_FINISHED = 2, FETCH_ADMI
 
 // Next unit of work for a lane: a cube to admit (admission ring, first), or a prefix item of a
 // queued iteration (work ring).  FETCH_FINISHED when nothing is queued, admitted or in flight.
-__device__ __forceinline__ int fetch_item(const SearchParams& P, uint32_t& slot, uint32_t& idx, uint32_t& plen,
-                                          uint32_t& bound, uint32_t& epoch) {
+__device__ __forceinline__ int fetch_item(const SearchParams& P, uint32_t seed, uint32_t& slot, uint32_t& idx,
+                                          uint32_t& plen, uint32_t& bound, uint32_t& epoch) {
     volatile QueueState* q = P.q;
     for (int tries = 0; tries < 64; ++tries) {
         if (q->yield) return FETCH_FINISHED;  // the host is stopping this launch
@@ -151,20 +151,31 @@ __device__ __forceinline__ int fetch_item(const SearchParams& P, uint32_t& slot,
         }
         unsigned long long h = q->head, t = q->tail;
         if (h >= t) return (q->active == 0u && q->admit_head >= q->admit_tail) ? FETCH_FINISHED : FETCH_EMPTY;
-        unsigned long long e = ((volatile unsigned long long*)P.ring)[h % P.ring_cap];
-        if ((e >> 32) != h / P.ring_cap) return FETCH_EMPTY;  // reserved, not yet written
-        uint32_t s = (uint32_t)e;
-        unsigned long long tk = atomicAdd(&P.slots[s].ticket, 1ull);
-        uint32_t i = (uint32_t)tk, pl = (uint32_t)(tk >> 56);
-        if (pl <= (uint32_t)MAX_PLEN && i < P.n_prefix[pl]) {
-            slot = s;
-            idx = i;
-            plen = pl;
-            bound = (uint32_t)(tk >> 48) & 0xFFu;
-            epoch = (uint32_t)(tk >> 32) & 0xFFFFu;
-            return FETCH_OK;
+        // Lanes spread over the first `spread` queued iterations, so each cube's items are worked
+        // roughly in order and a solution found early stops the rest of its last iteration.
+        unsigned long long span = t - h < P.spread ? t - h : P.spread;
+        unsigned long long pos = h + (seed + (uint32_t)tries) % span;
+        unsigned long long* cell = P.ring + pos % P.ring_cap;
+        unsigned long long e = *(volatile unsigned long long*)cell;
+        if ((e >> 32) != pos / P.ring_cap) {  // reserved, not yet written
+            if (pos == h) return FETCH_EMPTY;
+            continue;
         }
-        atomicCAS((unsigned long long*)&P.q->head, h, h + 1);  // this entry's iteration is handed out
+        uint32_t s = (uint32_t)e;
+        if (s != RING_RETIRED) {
+            unsigned long long tk = atomicAdd(&P.slots[s].ticket, 1ull);
+            uint32_t i = (uint32_t)tk, pl = (uint32_t)(tk >> 56);
+            if (pl <= (uint32_t)MAX_PLEN && i < P.n_prefix[pl]) {
+                slot = s;
+                idx = i;
+                plen = pl;
+                bound = (uint32_t)(tk >> 48) & 0xFFu;
+                epoch = (uint32_t)(tk >> 32) & 0xFFFFu;
+                return FETCH_OK;
+            }
+            atomicCAS(cell, e, (e & 0xFFFFFFFF00000000ull) | RING_RETIRED);  // its iteration is handed out
+        }
+        if (pos == h) atomicCAS((unsigned long long*)&P.q->head, h, h + 1);
     }
     return FETCH_EMPTY;
 }
@@ -218,6 +229,7 @@ __global__ void __launch_bounds__(THREADS) search_kernel(const DevTables* __rest
     bool have_item = false, done = false, idle = false;
     uint32_t iter = 0, idle_polls = 0, backoff = 32;
     const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lane_seed = (blockIdx.x * blockDim.x + threadIdx.x) * 0x9E3779B1u >> 7;
 
     for (;;) {
         bool eval = false;
@@ -254,7 +266,7 @@ __global__ void __launch_bounds__(THREADS) search_kernel(const DevTables* __rest
                 continue;
             }
             if (!have_item) {
-                int r = fetch_item(P, slot, idx, plen, bound, epoch);
+                int r = fetch_item(P, lane_seed, slot, idx, plen, bound, epoch);
                 if (r == FETCH_FINISHED) {
                     done = true;
                     break;

@@ -62,6 +62,7 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
     P->deeper_at[0] = (unsigned long long)(o && o->deeper_at0 > 0 ? o->deeper_at0 : 5e7);
     P->deeper_at[1] = (unsigned long long)(o && o->deeper_at1 > 0 ? o->deeper_at1 : 3e9);
     P->idle_limit = 1u << 21;  // ~8 s of idle polling (4 us back-off) before a warp leaves
+    P->spread = o && o->spread > 0 ? (uint32_t)o->spread : 128u;
     P->done_log = nullptr;
     P->done_log_cap = 0;
 }

@@ -110,6 +110,7 @@ typedef struct ccs_solve_opts {
     int blocks_per_sm;        /* persistent grid = blocks_per_sm * SMs (0: default)         */
     int threads;              /* threads per block: 128, 256 or 512 (0: default)            */
     double timeout_s;         /* give up after this long (0: no limit)                      */
+    int spread;               /* lanes work on up to this many queued cubes at once (0: 128) */
 } ccs_solve_opts;
 
 typedef struct ccs_result {

@@ -469,7 +469,7 @@ static int all_axes_tight(const uint32_t c[6], uint32_t budget) {
 
 static int dfs(search* S, const cube f[6], const uint32_t h[6], int g, int last) {
     if (g == S->bound) return is_solved(&f[0]);
-    if (S->stop && (S->nodes & 4095) == 0 && *S->stop) return 0;
+    if (S->stop && *S->stop) return 0;
     uint32_t budget = (uint32_t)(S->bound - g);
     int order[6];
     frame_order(h, budget, order);
