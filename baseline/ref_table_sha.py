@@ -2,7 +2,7 @@
 both sha256 digests in tests/golden/ref_table_sha256.json (the reference's table files are not
 distributed, so their bytes are pinned by running its code here).
 
-    python baseline/ref_table_sha.py [preset ...]     (default: every preset)
+    python baseline/ref_table_sha.py [--out FILE] [preset ...]     (default: every preset)
 """
 
 from __future__ import annotations
@@ -37,8 +37,8 @@ def sha_device(drv, ptr, nbytes) -> str:
     return h.hexdigest()
 
 
-def main(names):
-    out = json.loads(OUT.read_text()) if OUT.exists() else {}
+def main(names, out_path: Path = OUT):
+    out = json.loads(out_path.read_text()) if out_path.exists() else {}
     drv = ref_gpu.Driver(0)
     for name in names:
         p = kinds.PRESET_BY_NAME[name]
@@ -55,8 +55,12 @@ def main(names):
                      "reference_build_s": round(secs, 2), "libccs_sha256": mine_sha, "libccs_build_s": round(mine_s, 2),
                      "identical": ref_sha == mine_sha and counts == mine_counts}
         print(name, out[name], flush=True)
-        OUT.write_text(json.dumps(out, indent=1) + "\n")
+        out_path.write_text(json.dumps(out, indent=1) + "\n")
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or [p.name for p in kinds.PRESETS])
+    args = sys.argv[1:]
+    dest = OUT
+    if args[:1] == ["--out"]:
+        dest, args = Path(args[1]), args[2:]
+    main(args or [p.name for p in kinds.PRESETS], dest)

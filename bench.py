@@ -167,6 +167,39 @@ def cpu_arm(args, states, frames_words, table: np.ndarray, probes_per_cube: floa
             "probes_per_s": float(probes.sum()) / dt}
 
 
+def reference_gpu_arm(args, states, config) -> dict:
+    """The reference's own kernels.cu on this GPU (baseline/ref_gpu.py): its table build and its
+    per-bound host loop, the same cubes in chunks of ``--ref-batch`` (its CLI default is 100)."""
+
+    sys.path.insert(0, str(ROOT / "baseline"))
+    import ref_gpu
+
+    if not ref_gpu.available():
+        return {"impl": "reference-gpu", "unavailable": "baseline/_ref cubins not built (needs the reference checkout)"}
+    drv = ref_gpu.Driver(int(os.environ.get("LOCAL_RANK", "0")))
+    tables = ref_gpu.RefTables(drv, args.kind)
+    ptr, _, counts, build_s = tables.build(args.format)
+    solver = ref_gpu.RefSolver(drv, tables, ptr, args.format)
+    n = args.batch * args.steps
+    work = states[args.batch * args.warmup: args.batch * args.warmup + n]
+    solver.solve(states[: args.ref_batch])  # warm-up
+    t0 = time.perf_counter()
+    nodes = 0
+    lengths = []
+    for i in range(0, n, args.ref_batch):
+        for moves, nd, _ in solver.solve(work[i:i + args.ref_batch]):
+            nodes += nd
+            lengths.append(len(moves))
+    dt = time.perf_counter() - t0
+    return {"metric": METRIC, "value": n / dt, "unit": "cubes/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * dt / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8/u32 integer", "data": "synthetic", "config": config,
+            "impl": "reference-gpu", "nodes_per_cube": nodes / n, "table_build_s": build_s,
+            "lengths_histogram": {str(k): lengths.count(k) for k in sorted(set(lengths))},
+            "note": f"reference kernels.cu (unmodified, nvcc sm_100) driven with its host loop, {args.ref_batch} cubes "
+                    "per solve call, wall clock including its per-bound host round trips"}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -176,7 +209,8 @@ def main() -> None:
     ap.add_argument("--kind", default="d4t")
     ap.add_argument("--format", default="block", choices=["block", "b3"])
     ap.add_argument("--seed", type=int, default=2)
-    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference", "reference-gpu"])
+    ap.add_argument("--ref-batch", type=int, default=100, help="reference-gpu: cubes per solve call (its CLI default)")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
     ap.add_argument("--plain", type=int, default=32, help="cubes solved one per call for the plain numbers")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
@@ -194,6 +228,12 @@ def main() -> None:
                           f"{args.batch} cubes per step per GPU",
               "table": args.kind if args.format == "block" else f"{args.kind}-b3", "batch": args.batch,
               "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (7.8 GB table, random probes)"}
+
+    if args.impl == "reference-gpu":
+        if rank != 0:
+            return
+        print(json.dumps(reference_gpu_arm(args, my_states, config)))
+        return
 
     if args.impl == "reference":
         if rank != 0:

@@ -213,14 +213,97 @@ __device__ void admit_slot(const DevTables& T, const SearchParams& P, uint32_t s
     publish_epoch(P, s, next_plen(P, 0ull, bound), bound, 1u);
 }
 
-template <int MODE, int NEC, int FMT, int THREADS>
-__global__ void __launch_bounds__(THREADS) search_kernel(const DevTables* __restrict__ gT, SearchParams P) {
+// The six frames of a lane's current node: in registers (FramesReg) or in shared memory, word-major
+// with the lane index innermost so that every access of a warp is bank-conflict free (FramesSmem).
+struct FramesReg {
+    State f[6];
+    __device__ __forceinline__ void init(uint32_t*, int) {}
+    __device__ __forceinline__ State get(int k) const {
+        State t = f[0];
+#pragma unroll
+        for (int j = 1; j < 6; ++j)
+            if (k == j) t = f[j];
+        return t;
+    }
+    __device__ __forceinline__ State first() const { return f[0]; }
+    __device__ __forceinline__ void load(const uint32_t* src) {
+#pragma unroll
+        for (int j = 0; j < 6; ++j) f[j] = State{src[5 * j], src[5 * j + 1], src[5 * j + 2], src[5 * j + 3], src[5 * j + 4]};
+    }
+    __device__ __forceinline__ void step(const DevTables& T, int m) {
+#pragma unroll
+        for (int j = 0; j < 6; ++j) frame_do(T, f[j], j, m);
+    }
+    __device__ __forceinline__ void unstep(const DevTables& T, int m) {
+#pragma unroll
+        for (int j = 0; j < 6; ++j) frame_undo(T, f[j], j, m);
+    }
+};
+
+template <int THREADS>
+struct FramesSmem {
+    uint32_t* w;  // word i of frame k at w[(5 k + i) * THREADS]
+    __device__ __forceinline__ void init(uint32_t* base, int tid) { w = base + tid; }
+    __device__ __forceinline__ State get(int k) const {
+        const uint32_t* p = w + 5 * k * THREADS;
+        return State{p[0], p[THREADS], p[2 * THREADS], p[3 * THREADS], p[4 * THREADS]};
+    }
+    __device__ __forceinline__ void put(int k, const State& s) {
+        uint32_t* p = w + 5 * k * THREADS;
+        p[0] = s.c0;
+        p[THREADS] = s.c1;
+        p[2 * THREADS] = s.e0;
+        p[3 * THREADS] = s.e1;
+        p[4 * THREADS] = s.e2;
+    }
+    __device__ __forceinline__ State first() const { return get(0); }
+    __device__ __forceinline__ void load(const uint32_t* src) {
+#pragma unroll
+        for (int i = 0; i < 30; ++i) w[i * THREADS] = src[i];
+    }
+    __device__ __forceinline__ void step(const DevTables& T, int m) {
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            State t = get(j);
+            frame_do(T, t, j, m);
+            put(j, t);
+        }
+    }
+    __device__ __forceinline__ void unstep(const DevTables& T, int m) {
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            State t = get(j);
+            frame_undo(T, t, j, m);
+            put(j, t);
+        }
+    }
+};
+
+template <bool SMEM, int THREADS>
+struct FramesOf {
+    using type = FramesReg;
+};
+template <int THREADS>
+struct FramesOf<true, THREADS> {
+    using type = FramesSmem<THREADS>;
+};
+
+// Dynamic shared memory of a launch: the frames, when they live there.
+template <bool SMEM, int THREADS>
+constexpr size_t search_dyn_smem() {
+    return SMEM ? 30u * 4u * THREADS : 0u;
+}
+
+template <int MODE, int NEC, int FMT, int THREADS, bool SMEM, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) search_kernel(const DevTables* __restrict__ gT, SearchParams P) {
     __shared__ DevTables T;
+    extern __shared__ uint32_t frame_smem[];
     stage_tables(T, gT);
 
     unsigned char path[MAX_DEPTH];
     uint32_t hstack[MAX_DEPTH];
-    State f[6];
+    typename FramesOf<SMEM, THREADS>::type f;
+    f.init(frame_smem, threadIdx.x);
     uint32_t h = 0, c = 0;        // packed bounds of the node and of the child under evaluation
     uint32_t slot = 0, idx = 0, plen = 0, bound = 0, epoch = 0, pseq = 0;
     int g = 0, last = -1, m = -1, k = 0;
@@ -242,8 +325,7 @@ __global__ void __launch_bounds__(THREADS) search_kernel(const DevTables* __rest
                     break;
                 }
                 if (k == 6 && !all_axes_tight(c, bound - (uint32_t)g - 1u)) {  // push the surviving child
-#pragma unroll
-                    for (int j = 0; j < 6; ++j) frame_do(T, f[j], j, m);
+                    f.step(T, m);
                     hstack[g] = h;
                     path[g] = (unsigned char)m;
                     h = c;
@@ -251,7 +333,7 @@ __global__ void __launch_bounds__(THREADS) search_kernel(const DevTables* __rest
                     ++g;
                     if ((uint32_t)g == bound) {
                         Slot& sl = P.slots[slot];
-                        if (is_solved(f[0]) && atomicCAS(&sl.found, 0u, 1u) == 0u) {
+                        if (is_solved(f.first()) && atomicCAS(&sl.found, 0u, 1u) == 0u) {
                             sl.sol_len = (uint32_t)g;
                             for (int j = 0; j < g; ++j) sl.sol[j] = path[j];
                         }
@@ -286,10 +368,7 @@ __global__ void __launch_bounds__(THREADS) search_kernel(const DevTables* __rest
                     if (d == P.n_prefix[plen]) finish_slot(P, slot, SLOT_SOLVED);
                     continue;
                 }
-#pragma unroll
-                for (int j = 0; j < 6; ++j)
-                    f[j] = State{sl.frame[5 * j], sl.frame[5 * j + 1], sl.frame[5 * j + 2], sl.frame[5 * j + 3],
-                                 sl.frame[5 * j + 4]};
+f.load(sl.frame);
                 h = sl.h0;
                 pseq = plen ? __ldg(P.prefixes[plen] + idx) : 0u;
                 g = 0;
@@ -342,8 +421,7 @@ __global__ void __launch_bounds__(THREADS) search_kernel(const DevTables* __rest
             }
             --g;
             int pm = path[g];
-#pragma unroll
-            for (int j = 0; j < 6; ++j) frame_undo(T, f[j], j, pm);
+            f.unstep(T, pm);
             h = hstack[g];
             last = g > 0 ? path[g - 1] : -1;
             todo = (uint32_t)g < plen ? 0u
@@ -369,10 +447,7 @@ __global__ void __launch_bounds__(THREADS) search_kernel(const DevTables* __rest
         if (!eval) continue;
 
         // ---- one probe: frame k of child m ----
-        State t = f[0];
-#pragma unroll
-        for (int j = 1; j < 6; ++j)
-            if (k == j) t = f[j];
+        State t = f.get(k);
         if (k < 3) move_right(T, t, T.frame_move[k][m]);
         else move_left(T, t, T.inv_move[T.frame_move[k - 3][m]]);
         uint32_t v = probe_bound<MODE, NEC, FMT>(T, P, t);

@@ -24,7 +24,7 @@ using namespace ccs;
 namespace ccs {
 void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P);
 int grid_for(ccs_handle* h, const ccs_solve_opts* o);
-int launch_kernel(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream);
+int launch_kernel(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream, int variant);
 void make_slot(const uint32_t state[5], uint32_t request, Slot* s);
 void fill_result(const Slot& s, ccs_result* r);
 
@@ -109,7 +109,7 @@ int Server::step() {
     // 3. keep a search launch running while cubes are in flight
     if (kernel_running && cudaEventQuery(kernel_done) == cudaSuccess) kernel_running = false;
     if (!kernel_running && in_flight > 0) {
-        CCS_TRY(launch_kernel(h, P, grid, h->stream));
+        CCS_TRY(launch_kernel(h, P, grid, h->stream, opts.variant));
         CCS_CUDA_TRY(cudaEventRecord(kernel_done, h->stream));
         kernel_running = true;
     }

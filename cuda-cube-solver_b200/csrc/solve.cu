@@ -72,13 +72,24 @@ int grid_for(ccs_handle* h, const ccs_solve_opts* o) {
     return bps * h->sms;
 }
 
-int launch_kernel(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream) {
+// Launch shapes: frames in registers, 256 threads (variant 0), or frames in shared memory, 512
+// threads capped at 64 registers for 32 warps per SM (variant 1).
+template <int MODE, int NEC, int FMT, int THREADS, bool SMEM, int MINB>
+int launch_variant(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream) {
+    auto* k = search_kernel<MODE, NEC, FMT, THREADS, SMEM, MINB>;
+    constexpr size_t dyn = search_dyn_smem<SMEM, THREADS>();
+    if (dyn > 48 * 1024) CCS_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    k<<<grid, THREADS, dyn, stream>>>(h->d_tables, P);
+    CCS_CUDA_TRY(cudaGetLastError());
+    return CCS_OK;
+}
+
+int launch_kernel(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream, int variant) {
     return dispatch_kind(h->kind, [&](auto M, auto N) {
         return dispatch_fmt(h->format, [&](auto F) {
             constexpr int MODE = decltype(M)::value, NEC = decltype(N)::value, FMT = decltype(F)::value;
-            search_kernel<MODE, NEC, FMT, SEARCH_THREADS><<<grid, SEARCH_THREADS, 0, stream>>>(h->d_tables, P);
-            CCS_CUDA_TRY(cudaGetLastError());
-            return CCS_OK;
+            if (variant == 1) return launch_variant<MODE, NEC, FMT, 512, true, 2>(h, P, grid, stream);
+            return launch_variant<MODE, NEC, FMT, SEARCH_THREADS, false, 1>(h, P, grid, stream);
         });
     });
 }
@@ -142,7 +153,7 @@ extern "C" int ccs_solve(ccs_handle* h, const uint32_t* states, int n, const ccs
     unsigned long long prev_probes = ~0ull;
     for (;;) {
         CCS_CUDA_TRY(cudaEventRecord(h->ev0, st));
-        CCS_TRY(launch_kernel(h, P, grid, st));
+        CCS_TRY(launch_kernel(h, P, grid, st, opts ? opts->variant : 0));
         CCS_CUDA_TRY(cudaEventRecord(h->ev1, st));
         CCS_CUDA_TRY(cudaMemcpyAsync(&q, h->d_q, sizeof q, cudaMemcpyDeviceToHost, st));
         CCS_CUDA_TRY(cudaStreamSynchronize(st));

@@ -43,6 +43,7 @@ class SolveOpts(ctypes.Structure):
         ("threads", ctypes.c_int),
         ("timeout_s", ctypes.c_double),
         ("spread", ctypes.c_int),
+        ("variant", ctypes.c_int),
     ]
 
 
@@ -145,8 +146,9 @@ def kind_tables(kind: str) -> dict[str, np.ndarray]:
 
 
 def solve_opts(base_plen: int = 4, deeper_at: tuple[float, float] = (5e7, 3e9), blocks_per_sm: int = 0,
-               threads: int = 0, timeout_s: float = 0.0, spread: int = 0) -> SolveOpts:
-    return SolveOpts(base_plen, float(deeper_at[0]), float(deeper_at[1]), blocks_per_sm, threads, timeout_s, spread)
+               threads: int = 0, timeout_s: float = 0.0, spread: int = 0, variant: int = 0) -> SolveOpts:
+    return SolveOpts(base_plen, float(deeper_at[0]), float(deeper_at[1]), blocks_per_sm, threads, timeout_s, spread,
+                     variant)
 
 
 class Handle:

@@ -111,6 +111,7 @@ typedef struct ccs_solve_opts {
     int threads;              /* threads per block: 128, 256 or 512 (0: default)            */
     double timeout_s;         /* give up after this long (0: no limit)                      */
     int spread;               /* lanes work on up to this many queued cubes at once (0: 128) */
+    int variant;              /* search kernel variant: 0 frames in registers, 1 frames in shared memory */
 } ccs_solve_opts;
 
 typedef struct ccs_result {
