@@ -167,6 +167,50 @@ def cpu_arm(args, states, frames_words, table: np.ndarray, probes_per_cube: floa
             "probes_per_s": float(probes.sum()) / dt}
 
 
+def served_stream(args, solver, opts) -> dict:
+    """Config 5: Poisson arrivals (seed 3) into the continuous-batching server on the resident
+    table: 90% uniform cubes, 9% uniform cubes whose optimal length is >= 18, 1% superflips."""
+
+    from cuda_cube_solver import serving, workloads
+
+    n = args.serve
+    rng = np.random.default_rng(3)
+    pool = workloads.uniform_cubes(n + 200, seed=30)
+    hard_pool = workloads.uniform_cubes(4 * n // 10 + 16, seed=31)
+    lengths = [len(s.moves) for s in solver.solve(hard_pool)]  # set-up: find the long ones
+    hard = [c for c, L in zip(hard_pool, lengths) if L >= 18]
+    kinds_ = rng.choice(3, size=n, p=[0.90, 0.09, 0.01])
+    cubes, hi, ui = [], 0, 0
+    for k in kinds_:
+        if k == 2:
+            cubes.append(workloads.superflip())
+        elif k == 1 and hi < len(hard):
+            cubes.append(hard[hi])
+            hi += 1
+        else:
+            cubes.append(pool[ui])
+            ui += 1
+    arrivals = serving.poisson_arrivals(n, args.serve_rate, seed=3)
+    srv = serving.Server(solver.handle, 1024, opts)
+    try:
+        stats = serving.replay(srv, cubes, arrivals)
+    finally:
+        srv.close()
+    results = stats.pop("results")
+    from cuda_cube_solver.solver import verify_solutions
+    from cuda_cube_solver.device import state_words
+
+    assert verify_solutions(state_words(cubes), [r.moves for r in results])
+    stats.update({"mix": {"uniform": int((kinds_ == 0).sum()), "length_ge_18": int((kinds_ == 1).sum()),
+                          "superflip": int((kinds_ == 2).sum())},
+                  "rate_per_s": args.serve_rate, "table": config_table(args)})
+    return stats
+
+
+def config_table(args) -> str:
+    return args.kind if args.format == "block" else f"{args.kind}-b3"
+
+
 def reference_gpu_arm(args, states, config) -> dict:
     """The reference's own kernels.cu on this GPU (baseline/ref_gpu.py): its table build and its
     per-bound host loop, the same cubes in chunks of ``--ref-batch`` (its CLI default is 100)."""
@@ -214,6 +258,9 @@ def main() -> None:
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
     ap.add_argument("--plain", type=int, default=32, help="cubes solved one per call for the plain numbers")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--variant", type=int, default=0, help="search kernel variant (libccs ccs_solve_opts.variant)")
+    ap.add_argument("--serve", type=int, default=400, help="requests in the served-stream measurement (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=100.0, help="Poisson arrival rate of the served stream (/s)")
     args = ap.parse_args()
 
     world, rank, local = dist_setup()
@@ -258,6 +305,7 @@ def main() -> None:
     solver = GpuSolver.build_resident(args.kind, args.format, device=local)
     build_s = time.perf_counter() - t
     h = solver.handle
+    solver.variant = args.variant
     opts = solver._opts()
     batches = [state_words(my_states[i * args.batch:(i + 1) * args.batch]) for i in range(args.warmup + args.steps)]
 
@@ -307,6 +355,10 @@ def main() -> None:
                  "p50_s": float(np.percentile(plain_lat, 50)), "p99_s": float(np.percentile(plain_lat, 99)),
                  "worst_s": max(plain_lat)}
 
+    served = None
+    if args.serve:
+        served = served_stream(args, solver, opts)
+
     peaks = measured_peaks()
     total_probes = sum(probes)
     achieved = total_probes * SECTOR / (sum(kernel_ms) / 1000.0) / 1e9
@@ -336,7 +388,7 @@ def main() -> None:
                    "d2h_bytes_per_step": native.ctypes.sizeof(native.Result) * args.batch},
            "gpu_launches": int(sum(launches)),
            "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
-           "plain": plain, "table_build_s": build_s, "table_build_gpu_s": solver.build_seconds,
+           "plain": plain, "served": served, "table_build_s": build_s, "table_build_gpu_s": solver.build_seconds,
            "wall_s_per_step": statistics.mean(wall)}
     print(json.dumps(out))
     barrier(world)

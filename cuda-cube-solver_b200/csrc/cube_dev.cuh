@@ -143,16 +143,35 @@ __device__ __forceinline__ uint64_t table_index_dev(const DevTables& T, const ui
 // Table formats.
 enum Format : int { FMT_BLOCK = 0, FMT_B3 = 1 };
 
+// The whole 32-byte sector of a probe in one 256-bit load: one sector request instead of two
+// (the minimum and the offset word travel separately otherwise).  The table is read-only while
+// searching, so the load may be scheduled freely.
+__device__ __forceinline__ void load_sector(const uint32_t* p, uint32_t w[8]) {
+    asm("ld.global.nc.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7])
+                 : "l"(p));
+}
+
+__device__ __forceinline__ uint32_t pick8(const uint32_t w[8], uint32_t i) {
+    uint32_t r = w[0];
+#pragma unroll
+    for (uint32_t j = 1; j < 8; ++j)
+        if (i == j) r = w[j];
+    return r;
+}
+
 // Lower bound of entry idx.  Block: per 32-byte sector a u8 minimum then 124 two-bit offsets
 // (3 = at least minimum + 3) starting at bit 8.  Base 3: header m | cut << 6, then 155 digits,
 // five per byte (digit 0 = at least m, 1 = m + cut + 1, 2 = at least m + cut + 2).
 template <int FMT>
 __device__ __forceinline__ uint32_t lower_bound_dev(const uint32_t* __restrict__ tab, uint64_t idx) {
+    uint32_t w[8];
     if (FMT == FMT_B3) {
         uint64_t b = idx / 155u;
         uint32_t j = (uint32_t)(idx - b * 155u);
-        const unsigned char* p = reinterpret_cast<const unsigned char*>(tab) + b * 32u;
-        uint32_t hdr = __ldg(p), byte = __ldg(p + 1u + j / 5u);
+        load_sector(tab + b * 8u, w);
+        uint32_t q = 1u + j / 5u;
+        uint32_t hdr = w[0] & 0xFFu, byte = (pick8(w, q >> 2) >> (8u * (q & 3u))) & 0xFFu;
         uint32_t k = j % 5u;
         uint32_t pw = k == 0 ? 1u : k == 1 ? 3u : k == 2 ? 9u : k == 3 ? 27u : 81u;
         uint32_t d = (byte / pw) % 3u;
@@ -161,8 +180,8 @@ __device__ __forceinline__ uint32_t lower_bound_dev(const uint32_t* __restrict__
     } else {
         uint64_t b = idx / 124u;
         uint32_t pos = 8u + 2u * (uint32_t)(idx - b * 124u);
-        const uint32_t* p = tab + b * 8u;
-        return (__ldg(p) & 0xFFu) + ((__ldg(p + (pos >> 5)) >> (pos & 31u)) & 3u);
+        load_sector(tab + b * 8u, w);
+        return (w[0] & 0xFFu) + ((pick8(w, pos >> 5) >> (pos & 31u)) & 3u);
     }
 }
 

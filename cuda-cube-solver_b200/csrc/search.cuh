@@ -58,8 +58,11 @@ struct SearchParams {
     uint32_t n_prefix[MAX_PLEN + 1];
     uint32_t base_plen;              // prefix length of a cube's first iterations
     unsigned long long deeper_at[2]; // an iteration of at least this many nodes -> one move longer
+    unsigned long long shallow_at[2]; // an iteration of fewer nodes -> one move shorter (0: off)
     uint32_t idle_limit;             // idle polls before a warp leaves (kernel relaunched by the host)
     uint32_t spread;                 // lanes take items from up to this many queued iterations
+    uint32_t move_min;               // phased kernel: lanes waiting before a MOVE pass runs
+    uint32_t move_age;               // phased kernel: iterations a waiting lane may be deferred
     unsigned long long* done_log;    // host-mapped completion log (server), may be null
     uint32_t done_log_cap;
 };

@@ -120,11 +120,13 @@ __device__ __forceinline__ void finish_slot(const SearchParams& P, uint32_t s, u
     atomicSub(&P.q->active, 1u);
 }
 
-// Prefix length of the next iteration: base, plus one per threshold the last iteration reached
-// (a few huge subtrees would otherwise leave the GPU idle), at most the bound.
+// Prefix length of the next iteration: base, plus one per "deeper" threshold the last iteration
+// reached (a few huge subtrees would otherwise leave the GPU idle), minus one per "shallow"
+// threshold it stayed under (tiny items cost more to fetch than to search), at most the bound.
 __device__ __forceinline__ uint32_t next_plen(const SearchParams& P, unsigned long long last_nodes, uint32_t bound) {
     uint32_t pl = P.base_plen + (last_nodes >= P.deeper_at[0]) + (last_nodes >= P.deeper_at[1]);
-    pl = pl > (uint32_t)MAX_PLEN ? (uint32_t)MAX_PLEN : pl;
+    pl -= (uint32_t)(last_nodes < P.shallow_at[0]) + (uint32_t)(last_nodes < P.shallow_at[1]);
+    pl = pl < 1u ? 1u : (pl > (uint32_t)MAX_PLEN ? (uint32_t)MAX_PLEN : pl);
     return pl < bound ? pl : bound;
 }
 
@@ -135,7 +137,7 @@ enum FetchResult { FETCH_OK = 0, FETCH_EMPTY = 1, FETCH_FINISHED = 2, FETCH_ADMI
 __device__ __forceinline__ int fetch_item(const SearchParams& P, uint32_t seed, uint32_t& slot, uint32_t& idx,
                                           uint32_t& plen, uint32_t& bound, uint32_t& epoch) {
     volatile QueueState* q = P.q;
-    for (int tries = 0; tries < 64; ++tries) {
+    for (int tries = 0; tries < 8; ++tries) {
         if (q->yield) return FETCH_FINISHED;  // the host is stopping this launch
         unsigned long long ah = q->admit_head;
         if (ah < q->admit_tail) {
@@ -151,31 +153,34 @@ __device__ __forceinline__ int fetch_item(const SearchParams& P, uint32_t seed, 
         }
         unsigned long long h = q->head, t = q->tail;
         if (h >= t) return (q->active == 0u && q->admit_head >= q->admit_tail) ? FETCH_FINISHED : FETCH_EMPTY;
-        // Lanes spread over the first `spread` queued iterations, so each cube's items are worked
-        // roughly in order and a solution found early stops the rest of its last iteration.
-        unsigned long long span = t - h < P.spread ? t - h : P.spread;
-        unsigned long long pos = h + (seed + (uint32_t)tries) % span;
-        unsigned long long* cell = P.ring + pos % P.ring_cap;
-        unsigned long long e = *(volatile unsigned long long*)cell;
-        if ((e >> 32) != pos / P.ring_cap) {  // reserved, not yet written
-            if (pos == h) return FETCH_EMPTY;
-            continue;
-        }
-        uint32_t s = (uint32_t)e;
-        if (s != RING_RETIRED) {
-            unsigned long long tk = atomicAdd(&P.slots[s].ticket, 1ull);
-            uint32_t i = (uint32_t)tk, pl = (uint32_t)(tk >> 56);
-            if (pl <= (uint32_t)MAX_PLEN && i < P.n_prefix[pl]) {
-                slot = s;
-                idx = i;
-                plen = pl;
-                bound = (uint32_t)(tk >> 48) & 0xFFu;
-                epoch = (uint32_t)(tk >> 32) & 0xFFFFu;
-                return FETCH_OK;
+        // Lanes start at a seeded position among the first `spread` queued iterations and scan
+        // forward past handed-out entries, so the lanes spread over many cubes: each cube's items
+        // are worked roughly in prefix order and a solution found early stops the rest of its
+        // last iteration.
+        unsigned long long win = t - h < P.spread ? t - h : P.spread;
+        unsigned long long pos = h + (seed + (uint32_t)tries * 0x9E3779B1u) % win;
+        for (int step = 0; step < 32; ++step) {
+            unsigned long long* cell = P.ring + pos % P.ring_cap;
+            unsigned long long e = *(volatile unsigned long long*)cell;
+            if ((e >> 32) == pos / P.ring_cap) {  // written (unwritten or overwritten entries are skipped)
+                uint32_t s = (uint32_t)e;
+                if (s != RING_RETIRED) {
+                    unsigned long long tk = atomicAdd(&P.slots[s].ticket, 1ull);
+                    uint32_t i = (uint32_t)tk, pl = (uint32_t)(tk >> 56);
+                    if (pl <= (uint32_t)MAX_PLEN && i < P.n_prefix[pl]) {
+                        slot = s;
+                        idx = i;
+                        plen = pl;
+                        bound = (uint32_t)(tk >> 48) & 0xFFu;
+                        epoch = (uint32_t)(tk >> 32) & 0xFFFFu;
+                        return FETCH_OK;
+                    }
+                    atomicCAS(cell, e, (e & 0xFFFFFFFF00000000ull) | RING_RETIRED);  // iteration handed out
+                }
+                if (pos == h) atomicCAS((unsigned long long*)&P.q->head, h, h + 1);
             }
-            atomicCAS(cell, e, (e & 0xFFFFFFFF00000000ull) | RING_RETIRED);  // its iteration is handed out
+            if (++pos >= t) pos = h;
         }
-        if (pos == h) atomicCAS((unsigned long long*)&P.q->head, h, h + 1);
     }
     return FETCH_EMPTY;
 }

@@ -1,0 +1,208 @@
+// The IDA* search kernel, phase-ordered form.
+//
+// Same method, queue and per-lane depth-first search as search_kernel (search_kernel.cuh), but
+// the control between probes is a fixed sequence of predicated phases run once per warp
+// iteration -- RESOLVE the evaluated child, MOVE (push or pop), FINISH the item, FETCH the next
+// one, PICK the next child, PROBE one frame -- instead of a loop that each lane leaves at its own
+// pace.  Push and pop are the same work (a move applied to all six frames; pop uses the inverse
+// moves), so one MOVE pass serves every lane waiting for either, and it is deferred until enough
+// lanes wait (P.move_min), a few iterations passed (P.move_age) or no lane could probe: the
+// heaviest phase is then shared by many lanes instead of running for one.  Leaf survivors (child
+// at depth == threshold) are checked for a solution without a push.  Frames live in shared memory
+// (word-major, bank-conflict free), so the kernel fits 64 registers and 32 warps per SM.
+#pragma once
+
+#include "search_kernel.cuh"
+
+namespace ccs {
+
+template <int MODE, int NEC, int FMT, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevTables* __restrict__ gT, SearchParams P) {
+    __shared__ DevTables T;
+    extern __shared__ uint32_t frame_smem[];
+    stage_tables(T, gT);
+    FramesSmem<THREADS> f;
+    f.init(frame_smem, threadIdx.x);
+
+    unsigned char path[MAX_DEPTH];
+    uint32_t hstack[MAX_DEPTH];
+    uint32_t h = 0, c = 0, todo = 0, ord = 0, rem = 0;
+    uint32_t slot = 0, idx = 0, plen = 0, bound = 0, epoch = 0, pseq = 0;
+    int g = 0, m = -1, k = 0;
+    uint32_t nodes = 0, probes = 0;
+    bool have = false, done = false;
+    uint32_t iter = 0, idle_polls = 0, backoff = 32, fetches = 0, fetch_wait = 0;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lane_seed = (blockIdx.x * blockDim.x + threadIdx.x) * 0x9E3779B1u >> 7;
+
+    int mv = 0;  // frame update this lane waits for: 0 none, 1 push child m, 2 pop one level
+    uint32_t move_age = 0;
+    for (;;) {
+        // RESOLVE the child under evaluation: drop a pruned one, test a leaf survivor for a
+        // solution, and queue the push of an inner survivor.
+        if (m >= 0 && k >= 6 && mv == 0) {
+            if (k == 6 && !all_axes_tight(c, bound - (uint32_t)g - 1u)) {
+                if ((uint32_t)g + 1u == bound) {
+                    State t = f.get(0);
+                    frame_do(T, t, 0, m);
+                    Slot& sl = P.slots[slot];
+                    if (is_solved(t) && atomicCAS(&sl.found, 0u, 1u) == 0u) {
+                        sl.sol_len = (uint32_t)g + 1u;
+                        for (int j = 0; j < g; ++j) sl.sol[j] = path[j];
+                        sl.sol[g] = (uint8_t)m;
+                    }
+                } else {
+                    mv = 1;
+                }
+            }
+            if (mv == 0) m = -1;
+        }
+        // A node with no children left pops one level.
+        if (have && m < 0 && todo == 0u && g > 0 && mv == 0) mv = 2;
+        // MOVE: push and pop both apply a move to all six frames (pop with the inverse moves), so
+        // one pass serves every waiting lane; it runs once enough lanes wait, after a few
+        // iterations, or when no lane could probe meanwhile.
+        {
+            const unsigned want = __ballot_sync(0xFFFFFFFFu, mv != 0);
+            const unsigned ready = __ballot_sync(0xFFFFFFFFu, mv == 0 && ((m >= 0 && k < 6) || (have && todo != 0u)));
+            if (want && ((uint32_t)__popc(want) >= P.move_min || ++move_age >= P.move_age || ready == 0u)) {
+                move_age = 0;
+                if (mv) {
+                    const int mm = mv == 1 ? m : path[g - 1];
+#pragma unroll
+                    for (int j = 0; j < 6; ++j) {
+                        State t = f.get(j);
+                        if (j < 3) {
+                            int r = T.frame_move[j][mm];
+                            move_right(T, t, mv == 1 ? r : T.inv_move[r]);
+                        } else {
+                            int l = T.frame_move[j - 3][mm];
+                            move_left(T, t, mv == 1 ? T.inv_move[l] : l);
+                        }
+                        f.put(j, t);
+                    }
+                    if (mv == 1) {
+                        hstack[g] = h;
+                        path[g] = (unsigned char)m;
+                        h = c;
+                        ++g;
+                        uint32_t allow = (uint32_t)g < plen ? 1u << ((pseq >> (5 * g)) & 31u) : T.amask[m + 1];
+                        todo = allow & ~axis_move_mask(excluded_axes(h, bound - (uint32_t)g));
+                        ord = frame_order(h, bound - (uint32_t)g);
+                        m = -1;
+                    } else {
+                        --g;
+                        h = hstack[g];
+                        todo = 0u;
+                        if ((uint32_t)g >= plen) {
+                            int last = g > 0 ? path[g - 1] : -1;
+                            todo = T.amask[last + 1] & ~axis_move_mask(excluded_axes(h, bound - (uint32_t)g)) &
+                                   ~((2u << mm) - 1u);
+                            ord = frame_order(h, bound - (uint32_t)g);
+                        }
+                    }
+                    mv = 0;
+                }
+            }
+        }
+        // Solved elsewhere, or the host is stopping: drop the rest of the item.
+        if (have && mv == 0 && (++iter & 1023u) == 0u &&
+            (*(volatile uint32_t*)&P.slots[slot].found || ((volatile QueueState*)P.q)->yield)) {
+            todo = 0u;
+            g = 0;
+            m = -1;
+        }
+        // FINISH the item; the lane finishing an iteration's last item closes the iteration.
+        if (have && mv == 0 && m < 0 && todo == 0u && g == 0) {
+            Slot& sl = P.slots[slot];
+            atomicAdd(&sl.nodes, (unsigned long long)nodes);
+            atomicAdd(&sl.probes, (unsigned long long)probes);
+            atomicAdd(&sl.iter_nodes[bound < 24u ? bound : 23u], (unsigned long long)nodes);
+            atomicAdd(&P.q->probes, (unsigned long long)probes);
+            __threadfence();
+            uint32_t d = atomicAdd(&sl.done, 1u) + 1u;
+            if (d == P.n_prefix[plen]) {
+                __threadfence();
+                if (*(volatile uint32_t*)&sl.found) {
+                    finish_slot(P, slot, SLOT_SOLVED);
+                } else if (bound + 1u > MAX_BOUND) {
+                    atomicOr(&P.q->error, ERR_BOUND);
+                    finish_slot(P, slot, SLOT_ERROR);
+                } else {
+                    unsigned long long last_nodes = *(volatile unsigned long long*)&sl.iter_nodes[bound];
+                    publish_epoch(P, slot, next_plen(P, last_nodes, bound + 1u), bound + 1u, epoch + 1u);
+                }
+            }
+            have = false;
+        }
+        // FETCH the next item (or a cube to admit).
+        if (!have && !done && fetch_wait) {
+            --fetch_wait;  // the queue was empty: retry in a few iterations, not on every one
+        } else if (!have && !done) {
+            int r = fetch_item(P, lane_seed + (fetches++) * 0x2545F491u, slot, idx, plen, bound, epoch);
+            if (r == FETCH_EMPTY) fetch_wait = 16;
+            if (r == FETCH_FINISHED) {
+                done = true;
+            } else if (r == FETCH_ADMIT) {
+                admit_slot<MODE, NEC, FMT>(T, P, slot);
+            } else if (r == FETCH_OK) {
+                Slot& sl = P.slots[slot];
+                if (*(volatile uint32_t*)&sl.found) {  // solved by another item: count it done
+                    __threadfence();
+                    uint32_t d = atomicAdd(&sl.done, 1u) + 1u;
+                    if (d == P.n_prefix[plen]) finish_slot(P, slot, SLOT_SOLVED);
+                } else {
+                    f.load(sl.frame);
+                    h = sl.h0;
+                    pseq = plen ? __ldg(P.prefixes[plen] + idx) : 0u;
+                    g = 0;
+                    nodes = 0;
+                    probes = 0;
+                    uint32_t allow = plen ? 1u << (pseq & 31u) : T.amask[0];
+                    todo = allow & ~axis_move_mask(excluded_axes(h, bound));
+                    ord = frame_order(h, bound);
+                    have = true;
+                }
+            }
+        }
+        // PICK the next child.
+        if (have && mv == 0 && m < 0 && todo != 0u) {
+            m = __ffs(todo) - 1;
+            todo &= todo - 1;
+            ++nodes;
+            int inherit = 3 + (m / 3) % 3;  // inverse frame on the move's axis: same coset
+            c = h;
+            rem = ord & ~(0x41041u << inherit);
+            k = next_frame(rem);
+        }
+        if (__all_sync(0xFFFFFFFFu, done)) break;
+        const bool eval = mv == 0 && m >= 0 && k < 6;
+        if (__ballot_sync(0xFFFFFFFFu, eval || have) == 0u) {
+            // Nothing queued for this warp: back off; leave after too many empty polls in a row.
+            if (++idle_polls > P.idle_limit) {
+                if (lane == 0) atomicOr(&P.q->error, ERR_IDLE_LIMIT);
+                break;
+            }
+            __nanosleep(backoff);
+            backoff = backoff < 4096u ? backoff * 2u : 4096u;
+            continue;
+        }
+        idle_polls = 0;
+        backoff = 32;
+        // PROBE frame k of child m.
+        if (eval) {
+            State t = f.get(k);
+            if (k < 3) move_right(T, t, T.frame_move[k][m]);
+            else move_left(T, t, T.inv_move[T.frame_move[k - 3][m]]);
+            uint32_t v = probe_bound<MODE, NEC, FMT>(T, P, t);
+            ++probes;
+            uint32_t parent = hget(h, k);
+            if (k < 3 && parent) v = max(v, parent - 1u);  // a right move changes the coset distance by <= 1
+            v = v > 31u ? 31u : v;
+            c = hset(c, k, v);
+            k = ((uint32_t)g + 1u + v > bound) ? 7 : next_frame(rem);
+        }
+    }
+}
+
+}  // namespace ccs

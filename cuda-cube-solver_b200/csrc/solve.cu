@@ -8,6 +8,7 @@
 #include "ccs_internal.h"
 #include "dispatch.cuh"
 #include "search_kernel.cuh"
+#include "search_phased.cuh"
 
 using namespace ccs;
 
@@ -61,24 +62,42 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
     P->base_plen = (uint32_t)std::min(base, MAX_PLEN);
     P->deeper_at[0] = (unsigned long long)(o && o->deeper_at0 > 0 ? o->deeper_at0 : 5e7);
     P->deeper_at[1] = (unsigned long long)(o && o->deeper_at1 > 0 ? o->deeper_at1 : 3e9);
+    // Small iterations get shorter prefixes (fewer, larger items: fewer fetches); negative = off.
+    P->shallow_at[0] = (unsigned long long)(o && o->shallow_at0 != 0 ? (o->shallow_at0 > 0 ? o->shallow_at0 : 0) : 1e5);
+    P->shallow_at[1] = (unsigned long long)(o && o->shallow_at1 != 0 ? (o->shallow_at1 > 0 ? o->shallow_at1 : 0) : 1.5e6);
     P->idle_limit = 1u << 21;  // ~8 s of idle polling (4 us back-off) before a warp leaves
-    P->spread = o && o->spread > 0 ? (uint32_t)o->spread : 128u;
+    P->spread = o && o->spread > 0 ? (uint32_t)o->spread : 4096u;
+    P->move_min = o && o->move_min > 0 ? (uint32_t)o->move_min : 8u;
+    P->move_age = o && o->move_age > 0 ? (uint32_t)o->move_age : 4u;
     P->done_log = nullptr;
     P->done_log_cap = 0;
 }
 
 int grid_for(ccs_handle* h, const ccs_solve_opts* o) {
-    int bps = o && o->blocks_per_sm > 0 ? o->blocks_per_sm : 2;
+    int variant = o ? o->variant : 0;
+    int bps = o && o->blocks_per_sm > 0 ? o->blocks_per_sm : (variant == 1 ? 3 : 2);
     return bps * h->sms;
 }
 
-// Launch shapes: frames in registers, 256 threads (variant 0), or frames in shared memory, 512
-// threads capped at 64 registers for 32 warps per SM (variant 1).
+// Launch shapes: 0 (default) = phase-ordered control, frames in shared memory, 512 threads, 2
+// blocks per SM (32 warps, 64 registers); 1 = the same with 256 threads, 3 blocks per SM; 2 = loop
+// control, frames in registers, 256 threads, 2 blocks per SM; 3 = loop control, frames in shared
+// memory, 512 threads.
 template <int MODE, int NEC, int FMT, int THREADS, bool SMEM, int MINB>
 int launch_variant(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream) {
     auto* k = search_kernel<MODE, NEC, FMT, THREADS, SMEM, MINB>;
     constexpr size_t dyn = search_dyn_smem<SMEM, THREADS>();
-    if (dyn > 48 * 1024) CCS_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    if (dyn) CCS_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    k<<<grid, THREADS, dyn, stream>>>(h->d_tables, P);
+    CCS_CUDA_TRY(cudaGetLastError());
+    return CCS_OK;
+}
+
+template <int MODE, int NEC, int FMT, int THREADS, int MINB>
+int launch_phased(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream) {
+    auto* k = search_kernel_phased<MODE, NEC, FMT, THREADS, MINB>;
+    constexpr size_t dyn = search_dyn_smem<true, THREADS>();
+    if (dyn) CCS_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
     k<<<grid, THREADS, dyn, stream>>>(h->d_tables, P);
     CCS_CUDA_TRY(cudaGetLastError());
     return CCS_OK;
@@ -88,8 +107,10 @@ int launch_kernel(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t s
     return dispatch_kind(h->kind, [&](auto M, auto N) {
         return dispatch_fmt(h->format, [&](auto F) {
             constexpr int MODE = decltype(M)::value, NEC = decltype(N)::value, FMT = decltype(F)::value;
-            if (variant == 1) return launch_variant<MODE, NEC, FMT, 512, true, 2>(h, P, grid, stream);
-            return launch_variant<MODE, NEC, FMT, SEARCH_THREADS, false, 1>(h, P, grid, stream);
+            if (variant == 1) return launch_phased<MODE, NEC, FMT, 256, 3>(h, P, grid, stream);
+            if (variant == 2) return launch_variant<MODE, NEC, FMT, SEARCH_THREADS, false, 1>(h, P, grid, stream);
+            if (variant == 3) return launch_variant<MODE, NEC, FMT, 512, true, 2>(h, P, grid, stream);
+            return launch_phased<MODE, NEC, FMT, 512, 2>(h, P, grid, stream);
         });
     });
 }

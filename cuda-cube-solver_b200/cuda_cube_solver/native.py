@@ -44,6 +44,10 @@ class SolveOpts(ctypes.Structure):
         ("timeout_s", ctypes.c_double),
         ("spread", ctypes.c_int),
         ("variant", ctypes.c_int),
+        ("shallow_at0", ctypes.c_double),
+        ("shallow_at1", ctypes.c_double),
+        ("move_min", ctypes.c_int),
+        ("move_age", ctypes.c_int),
     ]
 
 
@@ -146,9 +150,10 @@ def kind_tables(kind: str) -> dict[str, np.ndarray]:
 
 
 def solve_opts(base_plen: int = 4, deeper_at: tuple[float, float] = (5e7, 3e9), blocks_per_sm: int = 0,
-               threads: int = 0, timeout_s: float = 0.0, spread: int = 0, variant: int = 0) -> SolveOpts:
+               threads: int = 0, timeout_s: float = 0.0, spread: int = 0, variant: int = 0,
+               shallow_at: tuple[float, float] = (0.0, 0.0), move_min: int = 0, move_age: int = 0) -> SolveOpts:
     return SolveOpts(base_plen, float(deeper_at[0]), float(deeper_at[1]), blocks_per_sm, threads, timeout_s, spread,
-                     variant)
+                     variant, float(shallow_at[0]), float(shallow_at[1]), move_min, move_age)
 
 
 class Handle:

@@ -107,7 +107,8 @@ class GpuSolver:
 
     ``prefix_len``: prefix length of the work items of a cube's first iterations; an iteration of
     at least ``deeper_prefix_at[i]`` nodes makes the next one use one move more.  ``grid`` is the
-    number of blocks of the persistent launch (default 2 per SM); ``block`` is fixed at 256.
+    number of blocks of the persistent launch (default: the library's choice for the kernel
+    variant); ``block`` is accepted for compatibility (the kernel's block size is fixed per variant).
     ``handle``: an already open ``native.Handle`` holding the table (``table_format`` and ``kind``
     must then describe it), e.g. one that built it with ``keep_resident``.
     """
@@ -118,8 +119,6 @@ class GpuSolver:
                  device: int = 0):
         if mode != "step" or not inverse:
             raise ValueError("only the step search with inverse frames is built (mode='step', inverse=True)")
-        if block != 256:
-            raise ValueError("block must be 256")
         tables = Path(tables)
         if tables.suffix == ".bin":
             tables = tables.parent
@@ -140,10 +139,12 @@ class GpuSolver:
         self.handle = handle
         sms = native.ctypes.c_int()
         native.check(native.lib.ccs_device_sms(handle.device, native.ctypes.byref(sms)))
-        self.grid = grid or 2 * sms.value
+        self.sms = sms.value
+        self.grid = grid  # None: the library's default for the kernel variant
         self.block = block
         self.last_kernel_ms = 0.0
         self.last_probes = 0
+        self.variant = 0  # search kernel variant (libccs); 0 is the fastest measured
 
     @classmethod
     def build_resident(cls, kind: str = "d4t", table_format: str = "block", log=None, device: int = 0, **kw):
@@ -156,10 +157,9 @@ class GpuSolver:
         return solver
 
     def _opts(self, timeout_s: float = 0.0) -> native.SolveOpts:
-        sms = native.ctypes.c_int()
-        native.check(native.lib.ccs_device_sms(self.handle.device, native.ctypes.byref(sms)))
-        blocks_per_sm = max(1, round(self.grid / sms.value))
-        return native.solve_opts(self.prefix_len, self.deeper_prefix_at[:2], blocks_per_sm, 256, timeout_s)
+        blocks_per_sm = max(1, round(self.grid / self.sms)) if self.grid else 0
+        return native.solve_opts(self.prefix_len, self.deeper_prefix_at[:2], blocks_per_sm, 0, timeout_s,
+                                 variant=self.variant)
 
     def root_h(self, states: list[CubieState]) -> tuple[np.ndarray, np.ndarray]:
         words = state_words(states)

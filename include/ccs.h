@@ -110,8 +110,12 @@ typedef struct ccs_solve_opts {
     int blocks_per_sm;        /* persistent grid = blocks_per_sm * SMs (0: default)         */
     int threads;              /* threads per block: 128, 256 or 512 (0: default)            */
     double timeout_s;         /* give up after this long (0: no limit)                      */
-    int spread;               /* lanes work on up to this many queued cubes at once (0: 128) */
-    int variant;              /* search kernel variant: 0 frames in registers, 1 frames in shared memory */
+    int spread;               /* lanes work on up to this many queued cubes at once (0: 4096) */
+    int variant;              /* search kernel variant (see solve.cu); 0: default                */
+    double shallow_at0;       /* an iteration of < this many nodes makes the next one use a    */
+    double shallow_at1;       /*   prefix one move shorter (0: 1e5 / 1.5e6, < 0: off)          */
+    int move_min;             /* lanes waiting before a frame-update pass runs (0: 8)          */
+    int move_age;             /* warp iterations a lane may wait for it (0: 4)                 */
 } ccs_solve_opts;
 
 typedef struct ccs_result {

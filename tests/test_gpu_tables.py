@@ -25,21 +25,31 @@ def _sha_golden():
     return json.loads(p.read_text()) if p.exists() else {}
 
 
+def _ref_sha():
+    """Digests of the tables the reference's own kernels build on a B200 (baseline/ref_table_sha.py)."""
+
+    p = GOLDEN / "ref_table_sha256.json"
+    return json.loads(p.read_text()) if p.exists() else {}
+
+
 def test_304_counts_and_bytes(depth_golden):
     h = resident_handle("304")
     assert h.build_counts == depth_golden["304"]["depth_counts"]
     assert h.table_bytes() == kinds.PRESET_BY_NAME["304"].table_bytes
-    ref = _sha_golden().get("304")
-    if ref:
-        assert _sha(h.table_copy()) == ref["block_sha256"]
+    digest = _sha(h.table_copy())
+    assert digest == _sha_golden()["304"]["block_sha256"]  # the CPU oracle's independent build
+    assert digest == _ref_sha()["304"]["reference_sha256"]  # the reference's own kernels
 
 
 @pytest.mark.parametrize("name", ["d4t", "d4"])
-def test_big_group_tables_counts(depth_golden, name):
+def test_big_group_tables_counts_and_bytes(depth_golden, name):
     h = resident_handle(name)
     assert h.build_counts == depth_golden[name]["depth_counts"]
     assert sum(h.build_counts) == depth_golden[name]["entries"]
     assert h.table_bytes() == kinds.PRESET_BY_NAME[name].table_bytes
+    ref = _ref_sha().get(name)
+    if ref:
+        assert _sha(h.table_copy()) == ref["reference_sha256"]
 
 
 def test_s4_b3_counts_and_bytes(depth_golden):
@@ -48,9 +58,7 @@ def test_s4_b3_counts_and_bytes(depth_golden):
         counts, _ = h.build_table("s4", "b3", None, keep_resident=True)
         assert counts == depth_golden["s4"]["depth_counts"]
         assert h.table_bytes() == kinds.PRESET_BY_NAME["s4-b3"].table_bytes
-        ref = _sha_golden().get("s4")
-        if ref:
-            assert _sha(h.table_copy()) == ref["b3_sha256"]
+        assert _sha(h.table_copy()) == _sha_golden()["s4"]["b3_sha256"]  # the CPU oracle's independent build
     finally:
         h.close()
 
