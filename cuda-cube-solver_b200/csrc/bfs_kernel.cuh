@@ -49,9 +49,7 @@ __device__ __forceinline__ uint32_t claim_with_stabilizer(const DevTables& T, co
     while (stab) {
         uint32_t t = __ffs(stab) - 1;
         stab &= stab - 1;
-        uint32_t e[3];
-        conj_edges(T, n, T.sym_mul[t][sym], e);
-        claimed += claim_entry(P.depth, base + edge_coord_dev<MODE, NEC>(T, e), d1);
+        claimed += claim_entry(P.depth, base + edge_coord_sym<MODE, NEC>(T, n, T.sym_mul[t][sym]), d1);
     }
     return claimed;
 }

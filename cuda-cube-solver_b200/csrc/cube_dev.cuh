@@ -5,9 +5,10 @@
 // class and symmetry from classidx, edge coordinate of the conjugated edges) and the block /
 // base-3 decoders of kernels.cu:396-434.  The formulation is this library's own: a U-D symmetry
 // keeps the E layer and maps the U and D layers onto themselves, so the position permutation of
-// an edge word is a single byte permute; masks are gathered with multiplies; E flips and non-E
-// flips come from one 256-entry table per word; the E-content class is read straight from the
-// 8-bit label string.
+// an edge word is a single byte permute and the cubie relabel reduces to a flip mask, a U/D swap
+// flag and a label-string table; masks are gathered with multiplies; E flips and non-E flips come
+// from one 256-entry table per word; the E-content class is read straight from the 8-bit label
+// string.
 #pragma once
 
 #include <cstdint>
@@ -86,43 +87,39 @@ __device__ __forceinline__ uint32_t corner_raw_dev(const DevTables& T, const Sta
     return twist * 70u + T.ccomb_rank[dmask];
 }
 
-// Edges conjugated by U-D symmetry sym.
-__device__ __forceinline__ void conj_edges(const DevTables& T, const State& s, int sym, uint32_t e[3]) {
-    uint32_t p[3];
-    p[0] = prmt(s.e0, s.e1, T.sy_psel[sym][0]);
-    p[1] = prmt(s.e0, s.e1, T.sy_psel[sym][1]);
-    p[2] = prmt(s.e2, s.e2, T.sy_psel[sym][2]);
-    const uint32_t r0 = T.sy_rel[sym][0], r1 = T.sy_rel[sym][1], r2 = T.sy_rel[sym][2];
-#pragma unroll
-    for (int w = 0; w < 3; ++w) {
-        uint32_t v = p[w];
-        uint32_t sel = nib_sel(v & 0x07070707u);
-        uint32_t hi = ((v >> 3) & 0x01010101u) * 0xFFu;
-        e[w] = ((prmt(r0, r1, sel) & ~hi) | (prmt(r2, r2, sel) & hi)) ^ (v & 0x10101010u) ^ T.sy_pflp[sym][w];
-    }
-}
-
-// Edge coordinate of conjugated edges e.  MODE KIND_GEN: (slice * 256 + non-E flips) * NEC +
-// class of the E content; KIND_304: (slice * 70 + U layout of the non-E positions) * 16 + E flips.
+// Edge coordinate of M_sym g M_sym^-1, computed without conjugating the cubie labels: a U-D
+// symmetry maps E cubies to E cubies and U cubies all to U or all to D, so after moving the bytes
+// to their conjugated positions (one prmt per word) the E mask is read directly, the flips need
+// one XOR (flip of E positions and of E cubies, T.sy_fx), the U mask at most a complement
+// (T.sy_swap), and the E labels one 256-entry relabel of the compacted label string (T.sy_lab).
+// MODE KIND_GEN: (slice * 256 + non-E flips) * NEC + class of the E content;
+// KIND_304: (slice * 70 + U layout of the non-E positions) * 16 + E flips.
 template <int MODE, int NEC>
-__device__ __forceinline__ uint32_t edge_coord_dev(const DevTables& T, const uint32_t e[3]) {
-    uint32_t em0 = gather4(e[0], 3), em1 = gather4(e[1], 3), em2 = gather4(e[2], 3);
-    uint32_t om0 = gather4(e[0], 4), om1 = gather4(e[1], 4), om2 = gather4(e[2], 4);
+__device__ __forceinline__ uint32_t edge_coord_sym(const DevTables& T, const State& s, int sym) {
+    uint32_t p0 = prmt(s.e0, s.e1, T.sy_psel[sym][0]);
+    uint32_t p1 = prmt(s.e0, s.e1, T.sy_psel[sym][1]);
+    uint32_t p2 = prmt(s.e2, s.e2, T.sy_psel[sym][2]);
+    uint32_t em0 = gather4(p0, 3), em1 = gather4(p1, 3), em2 = gather4(p2, 3);
+    uint32_t emask = em0 | (em1 << 4) | (em2 << 8);
+    uint32_t omask = gather4(p0, 4) | (gather4(p1, 4) << 4) | (gather4(p2, 4) << 8);
+    omask ^= (0xF00u ^ emask) & (0u - (uint32_t)T.sy_fx[sym]);
     uint32_t n0 = __popc(em0), n1 = __popc(em1);
-    uint32_t f0 = T.flp[(em0 << 4) | om0], f1 = T.flp[(em1 << 4) | om1], f2 = T.flp[(em2 << 4) | om2];
+    uint32_t f0 = T.flp[(em0 << 4) | (omask & 15u)], f1 = T.flp[(em1 << 4) | ((omask >> 4) & 15u)],
+             f2 = T.flp[(em2 << 4) | (omask >> 8)];
     uint32_t eflips = (f0 & 15u) | ((f1 & 15u) << n0) | ((f2 & 15u) << (n0 + n1));
-    uint32_t slice = T.slice_rank[em0 | (em1 << 4) | (em2 << 8)];
+    uint32_t slice = T.slice_rank[emask];
     if (MODE == KIND_304) {
-        uint32_t um0 = gather4(~(e[0] | (e[0] >> 1)), 2), um1 = gather4(~(e[1] | (e[1] >> 1)), 2),
-                 um2 = gather4(~(e[2] | (e[2] >> 1)), 2);
-        uint32_t u = T.ump[(em0 << 4) | um0] | (T.ump[(em1 << 4) | um1] << (4 - n0)) |
-                     (T.ump[(em2 << 4) | um2] << (8 - n0 - n1));
+        uint32_t umask = gather4(~(p0 | (p0 >> 1)), 2) | (gather4(~(p1 | (p1 >> 1)), 2) << 4) |
+                         (gather4(~(p2 | (p2 >> 1)), 2) << 8);
+        umask ^= 0xFFFu & (0u - (uint32_t)T.sy_swap[sym]);
+        uint32_t u = T.ump[(em0 << 4) | (umask & 15u)] | (T.ump[(em1 << 4) | ((umask >> 4) & 15u)] << (4 - n0)) |
+                     (T.ump[(em2 << 4) | (umask >> 8)] << (8 - n0 - n1));
         return (slice * 70u + T.ccomb_rank[u]) * 16u + eflips;
     } else {
         uint32_t nflips = (f0 >> 4) | ((f1 >> 4) << (4 - n0)) | ((f2 >> 4) << (8 - n0 - n1));
-        uint32_t eord = T.cmp4[em0][labels8(e[0])] | ((uint32_t)T.cmp4[em1][labels8(e[1])] << (2 * n0)) |
-                        ((uint32_t)T.cmp4[em2][labels8(e[2])] << (2 * (n0 + n1)));
-        return (slice * 256u + nflips) * (uint32_t)NEC + T.genc[(eord << 4) | eflips];
+        uint32_t eord = T.cmp4[em0][labels8(p0)] | ((uint32_t)T.cmp4[em1][labels8(p1)] << (2 * n0)) |
+                        ((uint32_t)T.cmp4[em2][labels8(p2)] << (2 * (n0 + n1)));
+        return (slice * 256u + nflips) * (uint32_t)NEC + T.genc[((uint32_t)T.sy_lab[sym][eord] << 4) | eflips];
     }
 }
 
@@ -135,9 +132,7 @@ template <int MODE, int NEC>
 __device__ __forceinline__ uint64_t table_index_dev(const DevTables& T, const uint32_t* __restrict__ classidx,
                                                     const State& s) {
     uint32_t packed = __ldg(classidx + corner_raw_dev(T, s));
-    uint32_t e[3];
-    conj_edges(T, s, packed & 15u, e);
-    return (uint64_t)(packed >> 4) * KindTraits<MODE, NEC>::N_EDGE + edge_coord_dev<MODE, NEC>(T, e);
+    return (uint64_t)(packed >> 4) * KindTraits<MODE, NEC>::N_EDGE + edge_coord_sym<MODE, NEC>(T, s, packed & 15u);
 }
 
 // Table formats.
@@ -147,9 +142,13 @@ enum Format : int { FMT_BLOCK = 0, FMT_B3 = 1 };
 // (the minimum and the offset word travel separately otherwise).  The table is read-only while
 // searching, so the load may be scheduled freely.
 __device__ __forceinline__ void load_sector(const uint32_t* p, uint32_t w[8]) {
+#ifdef CCS_HOST_EMULATION  // host build of this header for the CPU tests
+    for (int i = 0; i < 8; ++i) w[i] = p[i];
+#else
     asm("ld.global.nc.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                 : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7])
-                 : "l"(p));
+        : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7])
+        : "l"(p));
+#endif
 }
 
 __device__ __forceinline__ uint32_t pick8(const uint32_t w[8], uint32_t i) {
@@ -258,11 +257,13 @@ __device__ __forceinline__ void unrank_dev(const DevTables& T, const uint32_t* _
 }
 
 // Copy the constant tables into shared memory (whole block).
+#ifndef CCS_HOST_EMULATION
 __device__ __forceinline__ void stage_tables(DevTables& dst, const DevTables* __restrict__ src) {
     const uint4* s = reinterpret_cast<const uint4*>(src);
     uint4* d = reinterpret_cast<uint4*>(&dst);
     for (int i = threadIdx.x; i < (int)(sizeof(DevTables) / 16); i += blockDim.x) d[i] = s[i];
     __syncthreads();
 }
+#endif
 
 }  // namespace ccs

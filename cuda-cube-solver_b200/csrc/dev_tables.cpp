@@ -80,6 +80,20 @@ void build_dev_tables(const KindDesc& kind, DevTables* T) {
             T->sy_rel[s][w] = rel;
         }
         for (int t = 0; t < 16; ++t) T->sym_mul[t][s] = (uint8_t)ud_sym_mul(t, s);
+        // The relabel-free edge coordinate relies on these properties of U-D symmetries.
+        const int fx = a.eflip[8], swap = a.eperm[0] >= 4;
+        for (int p = 0; p < 12; ++p) {
+            if ((a.eperm[p] >= 8) != (p >= 8)) throw std::logic_error("U-D symmetry moves an E cubie out of the E layer");
+            if (a.eflip[p] != (p >= 8 ? fx : 0)) throw std::logic_error("U-D symmetry flips unevenly");
+            if (p < 8 && ((a.eperm[p] >= 4) != ((p >= 4) != (bool)swap))) throw std::logic_error("U-D symmetry splits a layer");
+        }
+        T->sy_fx[s] = (uint8_t)fx;
+        T->sy_swap[s] = (uint8_t)swap;
+        for (int v = 0; v < 256; ++v) {
+            uint32_t out = 0;
+            for (int j = 0; j < 4; ++j) out |= (uint32_t)(a.eperm[8 + ((v >> (2 * j)) & 3)] - 8) << (2 * j);
+            T->sy_lab[s][v] = (uint8_t)out;
+        }
     }
     for (int i = 0; i < 4096; ++i) T->slice_rank[i] = slice_rank()[i] == 0xFFFF ? 0 : slice_rank()[i];
     for (int i = 0; i < 495; ++i) T->slice_unrank[i] = slice_unrank()[i];

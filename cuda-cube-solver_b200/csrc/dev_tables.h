@@ -27,6 +27,12 @@ struct alignas(16) DevTables {
     uint32_t sy_psel[16][3];
     uint32_t sy_pflp[16][3];
     uint32_t sy_rel[16][3];
+    // What the cubie relabel of a U-D symmetry does to the coordinate: E cubies stay E cubies
+    // (labels permuted by sy_lab, on a compacted 2-bit label string), U cubies all become U or all
+    // become D (sy_swap), and the flips of E positions and of E cubies toggle together (sy_fx).
+    uint8_t sy_lab[16][256];
+    uint8_t sy_fx[16];
+    uint8_t sy_swap[16];
     uint16_t slice_rank[4096];   // 12-bit E mask -> 0..494
     uint16_t slice_unrank[496];
     uint16_t genc[4096];         // (E labels in position order, 8 bits) << 4 | E flips -> class

@@ -122,10 +122,12 @@ __device__ __forceinline__ void finish_slot(const SearchParams& P, uint32_t s, u
 
 // Prefix length of the next iteration: base, plus one per "deeper" threshold the last iteration
 // reached (a few huge subtrees would otherwise leave the GPU idle), minus one per "shallow"
-// threshold it stayed under (tiny items cost more to fetch than to search), at most the bound.
+// threshold it stayed under when many cubes are active (tiny items cost more to fetch than to
+// search, and other cubes fill the lanes), at most the bound.
 __device__ __forceinline__ uint32_t next_plen(const SearchParams& P, unsigned long long last_nodes, uint32_t bound) {
     uint32_t pl = P.base_plen + (last_nodes >= P.deeper_at[0]) + (last_nodes >= P.deeper_at[1]);
-    pl -= (uint32_t)(last_nodes < P.shallow_at[0]) + (uint32_t)(last_nodes < P.shallow_at[1]);
+    if (*(volatile uint32_t*)&P.q->active >= P.shallow_min_active)  // enough cubes to keep lanes busy
+        pl -= (uint32_t)(last_nodes < P.shallow_at[0]) + (uint32_t)(last_nodes < P.shallow_at[1]);
     pl = pl < 1u ? 1u : (pl > (uint32_t)MAX_PLEN ? (uint32_t)MAX_PLEN : pl);
     return pl < bound ? pl : bound;
 }

@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
             }
         }
         // Solved elsewhere, or the host is stopping: drop the rest of the item.
-        if (have && mv == 0 && (++iter & 1023u) == 0u &&
+        if (have && mv == 0 && (++iter & 255u) == 0u &&
             (*(volatile uint32_t*)&P.slots[slot].found || ((volatile QueueState*)P.q)->yield)) {
             todo = 0u;
             g = 0;

@@ -65,6 +65,7 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
     // Small iterations get shorter prefixes (fewer, larger items: fewer fetches); negative = off.
     P->shallow_at[0] = (unsigned long long)(o && o->shallow_at0 != 0 ? (o->shallow_at0 > 0 ? o->shallow_at0 : 0) : 1e5);
     P->shallow_at[1] = (unsigned long long)(o && o->shallow_at1 != 0 ? (o->shallow_at1 > 0 ? o->shallow_at1 : 0) : 1.5e6);
+    P->shallow_min_active = 32;
     P->idle_limit = 1u << 21;  // ~8 s of idle polling (4 us back-off) before a warp leaves
     P->spread = o && o->spread > 0 ? (uint32_t)o->spread : 4096u;
     P->move_min = o && o->move_min > 0 ? (uint32_t)o->move_min : 8u;
@@ -75,12 +76,12 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
 
 int grid_for(ccs_handle* h, const ccs_solve_opts* o) {
     int variant = o ? o->variant : 0;
-    int bps = o && o->blocks_per_sm > 0 ? o->blocks_per_sm : (variant == 1 ? 3 : 2);
+    int bps = o && o->blocks_per_sm > 0 ? o->blocks_per_sm : (variant == 0 ? 3 : 2);
     return bps * h->sms;
 }
 
-// Launch shapes: 0 (default) = phase-ordered control, frames in shared memory, 512 threads, 2
-// blocks per SM (32 warps, 64 registers); 1 = the same with 256 threads, 3 blocks per SM; 2 = loop
+// Launch shapes: 0 (default) = phase-ordered control, frames in shared memory, 256 threads, 3
+// blocks per SM (24 warps, 64 registers); 1 = the same with 512 threads, 2 blocks per SM; 2 = loop
 // control, frames in registers, 256 threads, 2 blocks per SM; 3 = loop control, frames in shared
 // memory, 512 threads.
 template <int MODE, int NEC, int FMT, int THREADS, bool SMEM, int MINB>
@@ -107,10 +108,10 @@ int launch_kernel(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t s
     return dispatch_kind(h->kind, [&](auto M, auto N) {
         return dispatch_fmt(h->format, [&](auto F) {
             constexpr int MODE = decltype(M)::value, NEC = decltype(N)::value, FMT = decltype(F)::value;
-            if (variant == 1) return launch_phased<MODE, NEC, FMT, 256, 3>(h, P, grid, stream);
+            if (variant == 1) return launch_phased<MODE, NEC, FMT, 512, 2>(h, P, grid, stream);
             if (variant == 2) return launch_variant<MODE, NEC, FMT, SEARCH_THREADS, false, 1>(h, P, grid, stream);
             if (variant == 3) return launch_variant<MODE, NEC, FMT, 512, true, 2>(h, P, grid, stream);
-            return launch_phased<MODE, NEC, FMT, 512, 2>(h, P, grid, stream);
+            return launch_phased<MODE, NEC, FMT, 256, 3>(h, P, grid, stream);
         });
     });
 }
