@@ -260,6 +260,7 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--variant", type=int, default=0, help="search kernel variant (libccs ccs_solve_opts.variant)")
     ap.add_argument("--serve", type=int, default=400, help="requests in the served-stream measurement (0: skip)")
+    ap.add_argument("--tune", action="store_true", help="autotune the kernel settings on a separate sample first")
     ap.add_argument("--serve-rate", type=float, default=100.0, help="Poisson arrival rate of the served stream (/s)")
     args = ap.parse_args()
 
@@ -306,7 +307,11 @@ def main() -> None:
     build_s = time.perf_counter() - t
     h = solver.handle
     solver.variant = args.variant
-    opts = solver._opts()
+    solver.use_autotune = False
+    tuned = None
+    if args.tune:  # set-up: its own cubes (seed + 1000), not the timed ones
+        tuned = solver.autotune(workloads.uniform_cubes(args.batch, seed=args.seed + 1000), save=False)
+    opts = solver._opts(n=args.batch)
     batches = [state_words(my_states[i * args.batch:(i + 1) * args.batch]) for i in range(args.warmup + args.steps)]
 
     for i in range(args.warmup):
@@ -387,6 +392,9 @@ def main() -> None:
            "e2e": {"value": e2e, "unit": "cubes/s", "h2d_bytes_per_step": 20 * args.batch,
                    "d2h_bytes_per_step": native.ctypes.sizeof(native.Result) * args.batch},
            "gpu_launches": int(sum(launches)),
+           "kernel_settings": {"variant": opts.variant, "base_plen": opts.base_plen, "spread": opts.spread,
+                               "move_min": opts.move_min, "move_age": opts.move_age,
+                               "autotuned": tuned is not None},
            "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
            "plain": plain, "served": served, "table_build_s": build_s, "table_build_gpu_s": solver.build_seconds,
            "wall_s_per_step": statistics.mean(wall)}

@@ -81,6 +81,10 @@ struct ccs_handle {
     int format = -1;
     uint32_t* d_table = nullptr;
     uint64_t table_bytes = 0;
+    // optional second resident table of a compatible kind (same class count and format)
+    std::string kind2_name;
+    uint32_t* d_table2 = nullptr;
+    uint64_t table2_bytes = 0;
     ccs::Slot* d_slots = nullptr;
     uint32_t slot_cap = 0;
     ccs::QueueState* d_q = nullptr;

@@ -157,6 +157,10 @@ void free_table(ccs_handle* h) {
     h->d_table = nullptr;
     h->table_bytes = 0;
     h->format = -1;
+    if (h->d_table2) cudaFree(h->d_table2);
+    h->d_table2 = nullptr;
+    h->table2_bytes = 0;
+    h->kind2_name.clear();
 }
 
 }  // namespace ccs

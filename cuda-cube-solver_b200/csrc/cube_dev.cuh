@@ -95,7 +95,7 @@ __device__ __forceinline__ uint32_t corner_raw_dev(const DevTables& T, const Sta
 // MODE KIND_GEN: (slice * 256 + non-E flips) * NEC + class of the E content;
 // KIND_304: (slice * 70 + U layout of the non-E positions) * 16 + E flips.
 template <int MODE, int NEC>
-__device__ __forceinline__ uint32_t edge_coord_sym(const DevTables& T, const State& s, int sym) {
+__device__ __forceinline__ uint32_t edge_coord_sym(const DevTables& T, const State& s, int sym, bool second = false) {
     uint32_t p0 = prmt(s.e0, s.e1, T.sy_psel[sym][0]);
     uint32_t p1 = prmt(s.e0, s.e1, T.sy_psel[sym][1]);
     uint32_t p2 = prmt(s.e2, s.e2, T.sy_psel[sym][2]);
@@ -119,7 +119,8 @@ __device__ __forceinline__ uint32_t edge_coord_sym(const DevTables& T, const Sta
         uint32_t nflips = (f0 >> 4) | ((f1 >> 4) << (4 - n0)) | ((f2 >> 4) << (8 - n0 - n1));
         uint32_t eord = T.cmp4[em0][labels8(p0)] | ((uint32_t)T.cmp4[em1][labels8(p1)] << (2 * n0)) |
                         ((uint32_t)T.cmp4[em2][labels8(p2)] << (2 * (n0 + n1)));
-        return (slice * 256u + nflips) * (uint32_t)NEC + T.genc[((uint32_t)T.sy_lab[sym][eord] << 4) | eflips];
+        const uint16_t* genc = second ? T.genc2 : T.genc;
+        return (slice * 256u + nflips) * (uint32_t)NEC + genc[((uint32_t)T.sy_lab[sym][eord] << 4) | eflips];
     }
 }
 
@@ -128,11 +129,12 @@ struct KindTraits {
     static constexpr uint64_t N_EDGE = MODE == KIND_304 ? 495ull * 70ull * 16ull : 495ull * 256ull * (uint64_t)NEC;
 };
 
+// second: index into the second resident table's kind (genc2).
 template <int MODE, int NEC>
 __device__ __forceinline__ uint64_t table_index_dev(const DevTables& T, const uint32_t* __restrict__ classidx,
-                                                    const State& s) {
+                                                    const State& s, bool second = false) {
     uint32_t packed = __ldg(classidx + corner_raw_dev(T, s));
-    return (uint64_t)(packed >> 4) * KindTraits<MODE, NEC>::N_EDGE + edge_coord_sym<MODE, NEC>(T, s, packed & 15u);
+    return (uint64_t)(packed >> 4) * KindTraits<MODE, NEC>::N_EDGE + edge_coord_sym<MODE, NEC>(T, s, packed & 15u, second);
 }
 
 // Table formats.

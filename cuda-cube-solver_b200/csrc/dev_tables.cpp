@@ -21,6 +21,15 @@ bool allowed_after(int last, int m) {
 }
 }  // namespace
 
+void build_genc(const KindDesc& kind, uint16_t genc[4096]) {
+    std::memset(genc, 0, 4096 * sizeof(uint16_t));
+    for (int e = 0; e < 256; ++e) {
+        uint8_t r = eorder_rank()[e];
+        if (r == 0xFF) continue;
+        for (int f = 0; f < 16; ++f) genc[(e << 4) | f] = kind.gen_class[r * 16 + f];
+    }
+}
+
 void build_dev_tables(const KindDesc& kind, DevTables* T) {
     std::memset(T, 0, sizeof(DevTables));
     for (int m = 0; m < 18; ++m) {
@@ -102,11 +111,8 @@ void build_dev_tables(const KindDesc& kind, DevTables* T) {
     for (int i = 0; i < 24; ++i) T->eorder_unrank[i] = eorder_unrank()[i];
     for (int i = 0; i < 256; ++i) T->eorder_rank[i] = eorder_rank()[i] == 0xFF ? 0 : eorder_rank()[i];
     if (kind.mode == KIND_GEN) {
-        for (int e = 0; e < 256; ++e) {
-            uint8_t r = eorder_rank()[e];
-            if (r == 0xFF) continue;
-            for (int f = 0; f < 16; ++f) T->genc[(e << 4) | f] = kind.gen_class[r * 16 + f];
-        }
+        build_genc(kind, T->genc);
+        std::memcpy(T->genc2, T->genc, sizeof(T->genc2));
         std::memcpy(T->gen_rep, kind.gen_rep, sizeof(T->gen_rep));
     }
     for (int m4 = 0; m4 < 16; ++m4)

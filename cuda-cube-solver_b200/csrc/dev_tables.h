@@ -36,6 +36,7 @@ struct alignas(16) DevTables {
     uint16_t slice_rank[4096];   // 12-bit E mask -> 0..494
     uint16_t slice_unrank[496];
     uint16_t genc[4096];         // (E labels in position order, 8 bits) << 4 | E flips -> class
+    uint16_t genc2[4096];        // the same for a second resident table of a compatible kind
     uint16_t gen_rep[2][384];    // class -> content (order rank * 16 + flips), by flip parity
     uint8_t cmp4[16][256];       // 2-bit fields of a byte selected by a 4-bit mask, compacted
     uint8_t flp[256];            // (E mask4 << 4 | flip mask4) -> E flips | non-E flips << 4
@@ -51,8 +52,12 @@ struct alignas(16) DevTables {
     uint32_t amask[20];          // canonical successors of last move (index last + 1), 18 bits
 };
 
-// Fills the tables for a kind (gen tables from KindDesc; unused for KIND_304).
+// Fills the tables for a kind (gen tables from KindDesc; unused for KIND_304); genc2 starts as a
+// copy of genc.
 void build_dev_tables(const KindDesc& kind, DevTables* out);
+
+// The E-content class table of a kind, as genc / genc2 hold it.
+void build_genc(const KindDesc& kind, uint16_t genc[4096]);
 
 }  // namespace ccs
 

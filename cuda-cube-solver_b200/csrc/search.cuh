@@ -27,6 +27,8 @@ struct alignas(16) Slot {
     unsigned long long nodes, probes;
     unsigned long long iter_nodes[24];  // nodes per bound
     unsigned long long t_admit, t_done; // device globaltimer, ns
+    uint32_t table;                  // 0: the handle's table, 1: its second resident table
+    uint32_t pad2[3];
 };
 
 struct QueueState {
@@ -54,6 +56,7 @@ struct SearchParams {
     uint32_t n_slots;
     const uint32_t* classidx;
     const uint32_t* table;           // solving table (block or base 3)
+    const uint32_t* table2;          // second resident table of a compatible kind (or = table)
     const uint32_t* prefixes[MAX_PLEN + 1];  // canonical move sequences, 5 bits per move
     uint32_t n_prefix[MAX_PLEN + 1];
     uint32_t base_plen;              // prefix length of a cube's first iterations

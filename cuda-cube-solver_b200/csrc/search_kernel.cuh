@@ -188,8 +188,9 @@ __device__ __forceinline__ int fetch_item(const SearchParams& P, uint32_t seed, 
 }
 
 template <int MODE, int NEC, int FMT>
-__device__ __forceinline__ uint32_t probe_bound(const DevTables& T, const SearchParams& P, const State& s) {
-    return lower_bound_dev<FMT>(P.table, table_index_dev<MODE, NEC>(T, P.classidx, s));
+__device__ __forceinline__ uint32_t probe_bound(const DevTables& T, const SearchParams& P, const State& s,
+                                                bool second = false) {
+    return lower_bound_dev<FMT>(second ? P.table2 : P.table, table_index_dev<MODE, NEC>(T, P.classidx, s, second));
 }
 
 // Admission of a new cube: root bounds of its six frames, first threshold, first iteration.
@@ -197,11 +198,12 @@ template <int MODE, int NEC, int FMT>
 __device__ void admit_slot(const DevTables& T, const SearchParams& P, uint32_t s) {
     Slot& sl = P.slots[s];
     State f0{sl.frame[0], sl.frame[1], sl.frame[2], sl.frame[3], sl.frame[4]};
+    const bool second = sl.table != 0u;
     uint32_t h = 0, bound = 0;
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
         State f{sl.frame[5 * k], sl.frame[5 * k + 1], sl.frame[5 * k + 2], sl.frame[5 * k + 3], sl.frame[5 * k + 4]};
-        uint32_t v = probe_bound<MODE, NEC, FMT>(T, P, f);
+        uint32_t v = probe_bound<MODE, NEC, FMT>(T, P, f, second);
         v = v > 31u ? 31u : v;
         h = hset(h, k, v);
         bound = v > bound ? v : bound;
@@ -316,7 +318,7 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel(const DevTables* 
     int g = 0, last = -1, m = -1, k = 0;
     uint32_t todo = 0, ord = 0, rem = 0;
     unsigned long long nodes = 0, probes = 0;
-    bool have_item = false, done = false, idle = false;
+    bool have_item = false, done = false, idle = false, second = false;
     uint32_t iter = 0, idle_polls = 0, backoff = 32;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lane_seed = (blockIdx.x * blockDim.x + threadIdx.x) * 0x9E3779B1u >> 7;
@@ -457,7 +459,7 @@ f.load(sl.frame);
         State t = f.get(k);
         if (k < 3) move_right(T, t, T.frame_move[k][m]);
         else move_left(T, t, T.inv_move[T.frame_move[k - 3][m]]);
-        uint32_t v = probe_bound<MODE, NEC, FMT>(T, P, t);
+        uint32_t v = probe_bound<MODE, NEC, FMT>(T, P, t, second);
         ++probes;
         uint32_t parent = hget(h, k);
         if (k < 3 && parent) v = max(v, parent - 1u);  // a right move changes the coset distance by <= 1

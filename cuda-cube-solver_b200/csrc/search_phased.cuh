@@ -30,7 +30,7 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
     uint32_t slot = 0, idx = 0, plen = 0, bound = 0, epoch = 0, pseq = 0;
     int g = 0, m = -1, k = 0;
     uint32_t nodes = 0, probes = 0;
-    bool have = false, done = false;
+    bool have = false, done = false, second = false;
     uint32_t iter = 0, idle_polls = 0, backoff = 32, fetches = 0, fetch_wait = 0;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lane_seed = (blockIdx.x * blockDim.x + threadIdx.x) * 0x9E3779B1u >> 7;
@@ -153,6 +153,7 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                     if (d == P.n_prefix[plen]) finish_slot(P, slot, SLOT_SOLVED);
                 } else {
                     f.load(sl.frame);
+                    second = sl.table != 0u;
                     h = sl.h0;
                     pseq = plen ? __ldg(P.prefixes[plen] + idx) : 0u;
                     g = 0;
@@ -194,7 +195,7 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
             State t = f.get(k);
             if (k < 3) move_right(T, t, T.frame_move[k][m]);
             else move_left(T, t, T.inv_move[T.frame_move[k - 3][m]]);
-            uint32_t v = probe_bound<MODE, NEC, FMT>(T, P, t);
+            uint32_t v = probe_bound<MODE, NEC, FMT>(T, P, t, second);
             ++probes;
             uint32_t parent = hget(h, k);
             if (k < 3 && parent) v = max(v, parent - 1u);  // a right move changes the coset distance by <= 1

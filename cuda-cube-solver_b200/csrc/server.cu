@@ -25,7 +25,7 @@ namespace ccs {
 void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P);
 int grid_for(ccs_handle* h, const ccs_solve_opts* o);
 int launch_kernel(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream, int variant);
-void make_slot(const uint32_t state[5], uint32_t request, Slot* s);
+void make_slot(const uint32_t state[5], uint32_t request, uint32_t table, Slot* s);
 void fill_result(const Slot& s, ccs_result* r);
 
 struct Server {
@@ -52,7 +52,7 @@ struct Server {
     int error = CCS_OK;
     std::string error_msg;
     uint64_t next_id = 1;
-    std::deque<std::pair<uint64_t, std::array<uint32_t, 5>>> pending;
+    std::deque<std::pair<uint64_t, std::array<uint32_t, 6>>> pending;  // state words, table id
     std::deque<std::pair<uint64_t, ccs_result>> finished;
     std::thread thread;
 
@@ -80,7 +80,7 @@ int Server::step() {
         ++consumed;
     }
     // 2. admissions
-    std::vector<std::pair<uint64_t, std::array<uint32_t, 5>>> take;
+    std::vector<std::pair<uint64_t, std::array<uint32_t, 6>>> take;
     {
         std::lock_guard<std::mutex> lock(mu);
         while (!pending.empty() && take.size() < free_slots.size()) {
@@ -94,7 +94,7 @@ int Server::step() {
             free_slots.pop_back();
             slot_request[s] = t.first;
             Slot sl;
-            make_slot(t.second.data(), (uint32_t)t.first, &sl);
+            make_slot(t.second.data(), (uint32_t)t.first, t.second[5], &sl);
             CCS_CUDA_TRY(cudaMemcpyAsync(h->d_slots + s, &sl, sizeof sl, cudaMemcpyHostToDevice, copy));
             unsigned long long pos = admit_pos++;
             unsigned long long entry = ((pos / P.admit_cap) << 32) | s;
@@ -193,12 +193,19 @@ extern "C" int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* 
 }
 
 extern "C" int ccs_server_submit(ccs_handle* h, const uint32_t* state, uint64_t* request_id) {
+    return ccs_server_submit_table(h, state, 0, request_id);
+}
+
+extern "C" int ccs_server_submit_table(ccs_handle* h, const uint32_t* state, int table_id, uint64_t* request_id) {
     if (!h || !state) return fail(CCS_E_ARG, "NULL argument");
     Server* s = h->server;
     if (!s) return fail(CCS_E_STATE, "server not running");
     if (!is_legal(unpack(state))) return fail(CCS_E_ARG, "not a legal position");
-    std::array<uint32_t, 5> st;
+    if (table_id < 0 || table_id > 1 || (table_id == 1 && !h->d_table2))
+        return fail(CCS_E_ARG, "table id %d: 0, or 1 with a second table attached", table_id);
+    std::array<uint32_t, 6> st;
     std::memcpy(st.data(), state, 20);
+    st[5] = (uint32_t)table_id;
     {
         std::lock_guard<std::mutex> lock(s->mu);
         if (s->stop) return fail(s->error ? s->error : CCS_E_STATE, "server stopped: %s", s->error_msg.c_str());

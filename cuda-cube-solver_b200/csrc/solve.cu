@@ -54,6 +54,7 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
     P->n_slots = h->slot_cap;
     P->classidx = h->d_classidx;
     P->table = h->d_table;
+    P->table2 = h->d_table2 ? h->d_table2 : h->d_table;
     for (int L = 0; L <= MAX_PLEN; ++L) {
         P->prefixes[L] = h->d_prefix[L];
         P->n_prefix[L] = h->n_prefix[L];
@@ -118,12 +119,13 @@ int launch_kernel(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t s
 
 // Host slot record for a new cube: frames, no iteration yet (the admitting lane computes the
 // root bounds and publishes the first one).
-void make_slot(const uint32_t state[5], uint32_t request, Slot* s) {
+void make_slot(const uint32_t state[5], uint32_t request, uint32_t table, Slot* s) {
     std::memset(s, 0, sizeof *s);
     cube_frames(state, s->frame);
     s->status = SLOT_ACTIVE;
     s->ticket = TICKET_IDLE;
     s->request = request;
+    s->table = table;
 }
 
 void fill_result(const Slot& s, ccs_result* r) {
@@ -145,15 +147,24 @@ void fill_result(const Slot& s, ccs_result* r) {
 }  // namespace ccs
 
 extern "C" int ccs_solve(ccs_handle* h, const uint32_t* states, int n, const ccs_solve_opts* opts, ccs_result* results) {
+    return ccs_solve_tables(h, states, nullptr, n, opts, results);
+}
+
+extern "C" int ccs_solve_tables(ccs_handle* h, const uint32_t* states, const uint8_t* table_ids, int n,
+                                const ccs_solve_opts* opts, ccs_result* results) {
     if (!h || (n > 0 && (!states || !results))) return fail(CCS_E_ARG, "NULL argument");
     if (!h->d_table) return fail(CCS_E_STATE, "no table loaded");
+    for (int i = 0; table_ids && i < n; ++i) {
+        if (table_ids[i] > 1) return fail(CCS_E_ARG, "table id %d of cube %d is not 0 or 1", table_ids[i], i);
+        if (table_ids[i] == 1 && !h->d_table2) return fail(CCS_E_STATE, "cube %d asks for a second table; none attached", i);
+    }
     if (h->server) return fail(CCS_E_STATE, "the server owns this handle's search buffers");
     if (n <= 0) return CCS_OK;
     for (int i = 0; i < n; ++i)
         if (!is_legal(unpack(states + 5ull * i))) return fail(CCS_E_ARG, "cube %d is not a legal position", i);
     CCS_TRY(ensure_search_buffers(h, (uint32_t)n));
     std::vector<Slot> host(n);
-    for (int i = 0; i < n; ++i) make_slot(states + 5ull * i, (uint32_t)i, &host[i]);
+    for (int i = 0; i < n; ++i) make_slot(states + 5ull * i, (uint32_t)i, table_ids ? table_ids[i] : 0u, &host[i]);
     std::vector<unsigned long long> admit(n);
     for (int i = 0; i < n; ++i) admit[i] = (unsigned long long)i;  // lap 0
     QueueState q;

@@ -4,6 +4,7 @@
 #include <chrono>
 #include <cstdarg>
 #include <cstdio>
+#include <cstddef>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -113,6 +114,65 @@ extern "C" int ccs_load_table(ccs_handle* h, const char* kind, int format, const
     return CCS_OK;
 }
 
+// The second resident table: same kind family as the first (class count, format), so one search
+// kernel serves both; only the E-content class table (genc2) and the table pointer differ.
+static int attach_second(ccs_handle* h, const char* kind, int format, uint32_t* d, uint64_t bytes) {
+    KindDesc k2;
+    CCS_TRY(get_kind(kind, &k2));
+    if (!h->d_table || h->format != format || k2.mode != h->kind.mode || k2.nec != h->kind.nec)
+        return fail(CCS_E_ARG, "a second table must match the first one's kind family and format");
+    uint16_t genc[4096];
+    build_genc(k2, genc);
+    CCS_CUDA_TRY(cudaMemcpy(reinterpret_cast<char*>(h->d_tables) + offsetof(DevTables, genc2), genc, sizeof genc,
+                            cudaMemcpyHostToDevice));
+    if (h->d_table2) cudaFree(h->d_table2);
+    h->d_table2 = d;
+    h->table2_bytes = bytes;
+    h->kind2_name = kind;
+    return CCS_OK;
+}
+
+extern "C" int ccs_attach_table(ccs_handle* h, const char* kind, int format, const char* path) {
+    if (!h || !kind || !path) return fail(CCS_E_ARG, "NULL argument");
+    if (!h->d_table) return fail(CCS_E_STATE, "load or build the first table before attaching a second one");
+    KindDesc k2;
+    CCS_TRY(get_kind(kind, &k2));
+    uint64_t want = table_bytes_for(k2, format);
+    const std::string path_s(path);
+    FILE* f = fopen(path_s.c_str(), "rb");
+    if (!f) return fail(CCS_E_FILE, "%s not found", path_s.c_str());
+    fseek(f, 0, SEEK_END);
+    long long size = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    if (size < 0 || (uint64_t)size != want) {
+        fclose(f);
+        return fail(CCS_E_FILE, "%s: size %lld, expected %llu", path_s.c_str(), size, (unsigned long long)want);
+    }
+    CCS_CUDA_TRY(cudaSetDevice(h->device));
+    uint32_t* d = nullptr;
+    if (cudaMalloc(&d, want) != cudaSuccess) {
+        fclose(f);
+        return fail(CCS_E_NOMEM, "device allocation of %llu bytes for the second table", (unsigned long long)want);
+    }
+    PinnedBuffer buf(CHUNK_BYTES);
+    for (uint64_t off = 0; buf.p && off < want; off += CHUNK_BYTES) {
+        size_t n = (size_t)std::min<uint64_t>(CHUNK_BYTES, want - off);
+        if (fread(buf.p, 1, n, f) != n || cudaMemcpy((char*)d + off, buf.p, n, cudaMemcpyHostToDevice) != cudaSuccess) {
+            fclose(f);
+            cudaFree(d);
+            return fail(CCS_E_FILE, "%s: read or copy failed", path_s.c_str());
+        }
+    }
+    fclose(f);
+    if (!buf.p) {
+        cudaFree(d);
+        return fail(CCS_E_NOMEM, "pinned staging buffer");
+    }
+    int rc = attach_second(h, kind, format, d, want);
+    if (rc != CCS_OK) cudaFree(d);
+    return rc;
+}
+
 extern "C" int ccs_build_table(ccs_handle* h, const char* kind, int format, const char* out_path, int keep_resident,
                                uint64_t* depth_counts, int max_depths, int* n_depths, double* seconds,
                                ccs_log_fn log) {
@@ -125,7 +185,10 @@ extern "C" int ccs_build_table(ccs_handle* h, const char* kind, int format, cons
     const uint64_t n_chunks = (n_entries + 15) / 16;
     auto t0 = std::chrono::steady_clock::now();
 
-    if (keep_resident) free_table(h);  // make room; the new table replaces it
+    // keep_resident 1: the new table replaces the handle's tables; 2: it becomes the second table.
+    std::string first_kind = h->kind_name;
+    if (keep_resident == 2 && !h->d_table) return fail(CCS_E_STATE, "no first table to attach a second one to");
+    if (keep_resident == 1) free_table(h);
     DeviceBuffer<uint8_t> depth(n_chunks * 16);
     DeviceBuffer<unsigned long long> counter(40);
     if (!depth.ok() || !counter.ok())
@@ -230,11 +293,16 @@ extern "C" int ccs_build_table(ccs_handle* h, const char* kind, int format, cons
 
     int rc = CCS_OK;
     if (out_path) rc = write_device_file(d_out, out_bytes, out_path, h->stream);
-    if (rc == CCS_OK && keep_resident) {
+    if (rc == CCS_OK && keep_resident == 1) {
         free_table(h);
         h->d_table = d_out;
         h->table_bytes = out_bytes;
         h->format = format;
+    } else if (rc == CCS_OK && keep_resident == 2) {
+        std::string second = h->kind_name;
+        rc = set_kind(h, first_kind.c_str());  // the constants stay those of the first table's kind
+        if (rc == CCS_OK) rc = attach_second(h, second.c_str(), format, d_out, out_bytes);
+        if (rc != CCS_OK) cudaFree(d_out);
     } else {
         cudaFree(d_out);
     }

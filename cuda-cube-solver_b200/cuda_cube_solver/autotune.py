@@ -1,0 +1,105 @@
+"""Autotuner for the batched search: picks the launch settings of libccs's search kernel for a
+GPU, table and batch size by measuring them.
+
+Knobs (``native.SolveOpts``):
+
+* ``variant``: block shape -- 0 = 256 threads x 3 blocks per SM (24 warps), 1 = 512 x 2 (32 warps);
+* ``base_plen``: cut depth of the work items (prefix length of a cube's iterations);
+* ``move_min`` / ``move_age``: how many lanes wait, and for how many iterations, before the
+  frame-update pass (push / pop) runs -- the depth of the lanes' update pipeline;
+* ``spread``: over how many queued cubes the lanes spread.
+
+Coordinate descent from the library defaults: each knob in turn takes the value with the best
+device time on the sample (the same cubes every time), twice round.  Results are cached in a JSON
+file keyed by GPU name, table and batch-size bucket, and ``GpuSolver`` picks them up.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+import time
+from pathlib import Path
+
+from cuda_cube_solver import native
+from cuda_cube_solver.device import state_words
+
+CACHE = Path(os.environ.get("CCS_TUNE_CACHE", Path.home() / ".cache" / "cuda_cube_solver" / "autotune.json"))
+
+SPACE = {
+    "variant": [0, 1],
+    "base_plen": [3, 4, 5],
+    "move": [(4, 2), (8, 4), (12, 6), (16, 8)],
+    "spread": [512, 1024, 4096],
+}
+DEFAULT = {"variant": 0, "base_plen": 4, "move": (8, 4), "spread": 4096}
+
+
+def opts_of(cfg: dict, timeout_s: float = 600.0) -> native.SolveOpts:
+    return native.solve_opts(base_plen=cfg["base_plen"], variant=cfg["variant"], spread=cfg["spread"],
+                             move_min=cfg["move"][0], move_age=cfg["move"][1], timeout_s=timeout_s)
+
+
+def batch_bucket(n: int) -> str:
+    return "1" if n <= 1 else ("small" if n < 64 else ("medium" if n < 1024 else "large"))
+
+
+def _key(gpu: str, table: str, n: int) -> str:
+    return f"{gpu}|{table}|{batch_bucket(n)}"
+
+
+def measure(handle: native.Handle, words, cfg: dict) -> float:
+    """Device seconds of one batched solve of ``words`` with ``cfg``."""
+
+    handle.solve(words, opts_of(cfg))
+    return handle.last_solve_stats()[0] / 1000.0
+
+
+def tune(handle: native.Handle, states, table: str, rounds: int = 2, log=None) -> dict:
+    """Best settings for ``states`` (a representative sample) on the handle's table."""
+
+    words = state_words(states)
+    best = dict(DEFAULT)
+    measure(handle, words, best)  # warm-up
+    best_t = measure(handle, words, best)
+    trials = [(dict(best), best_t)]
+    for _ in range(rounds):
+        for knob, values in SPACE.items():
+            for v in values:
+                if v == best[knob]:
+                    continue
+                cfg = dict(best, **{knob: v})
+                t = measure(handle, words, cfg)
+                trials.append((cfg, t))
+                if log:
+                    log(f"{knob}={v}: {len(states) / t:8.1f} cubes/s")
+                if t < best_t:
+                    best, best_t = cfg, t
+    return {"config": best, "cubes_per_s": len(states) / best_t, "trials": len(trials),
+            "default_cubes_per_s": len(states) / trials[0][1], "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
+
+
+def gpu_name(device: int = 0) -> str:
+    try:
+        import torch
+
+        return torch.cuda.get_device_name(device)
+    except Exception:
+        return "cuda"
+
+
+def save(result: dict, table: str, n: int, device: int = 0) -> None:
+    CACHE.parent.mkdir(parents=True, exist_ok=True)
+    data = json.loads(CACHE.read_text()) if CACHE.exists() else {}
+    data[_key(gpu_name(device), table, n)] = result
+    CACHE.write_text(json.dumps(data, indent=1) + "\n")
+
+
+def lookup(table: str, n: int, device: int = 0) -> dict | None:
+    if not CACHE.exists():
+        return None
+    cfg = json.loads(CACHE.read_text()).get(_key(gpu_name(device), table, n))
+    if cfg:
+        cfg = dict(cfg["config"])
+        cfg["move"] = tuple(cfg["move"])
+    return cfg

@@ -87,7 +87,12 @@ _SIGS = {
     "ccs_lower_bound": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p],
     "ccs_root_bounds": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p],
     "ccs_solve": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _P(SolveOpts), ctypes.c_void_p],
+    "ccs_solve_tables": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _P(SolveOpts), ctypes.c_void_p],
+    "ccs_attach_table": [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p],
+    "ccs_server_submit_table": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _P(ctypes.c_uint64)],
     "ccs_last_solve_stats": [ctypes.c_void_p, _P(ctypes.c_double), _P(ctypes.c_uint64), _P(ctypes.c_int)],
+    "ccs_gather_bench": [ctypes.c_int, ctypes.c_uint64, ctypes.c_int, _P(ctypes.c_double), _P(ctypes.c_double)],
+    "ccs_probe_bench": [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _P(ctypes.c_double), _P(ctypes.c_double)],
     "ccs_server_start": [ctypes.c_void_p, ctypes.c_int, _P(SolveOpts)],
     "ccs_server_submit": [ctypes.c_void_p, ctypes.c_void_p, _P(ctypes.c_uint64)],
     "ccs_server_poll": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, _P(ctypes.c_int)],
@@ -149,6 +154,14 @@ def kind_tables(kind: str) -> dict[str, np.ndarray]:
     return out
 
 
+def gather_bench(device: int = 0, nbytes: int = 8 << 30, rounds: int = 64) -> tuple[float, float]:
+    """(random 32-byte sectors per second, ms) over an ``nbytes`` device buffer."""
+
+    rate, ms = ctypes.c_double(), ctypes.c_double()
+    check(lib.ccs_gather_bench(device, nbytes, rounds, ctypes.byref(rate), ctypes.byref(ms)))
+    return rate.value, ms.value
+
+
 def solve_opts(base_plen: int = 4, deeper_at: tuple[float, float] = (5e7, 3e9), blocks_per_sm: int = 0,
                threads: int = 0, timeout_s: float = 0.0, spread: int = 0, variant: int = 0,
                shallow_at: tuple[float, float] = (0.0, 0.0), move_min: int = 0, move_age: int = 0) -> SolveOpts:
@@ -181,7 +194,8 @@ class Handle:
     def load_table(self, kind: str, fmt: str, path) -> None:
         check(lib.ccs_load_table(self._h, kind.encode(), FORMATS[fmt], str(path).encode()))
 
-    def build_table(self, kind: str, fmt: str, out_path=None, keep_resident: bool = False, log=None):
+    def build_table(self, kind: str, fmt: str, out_path=None, keep_resident: int = 0, log=None):
+        """keep_resident: 0 drop, 1 keep as the table, 2 keep as the second (attached) table."""
         counts = np.zeros(64, np.uint64)
         n = ctypes.c_int()
         secs = ctypes.c_double()
@@ -226,12 +240,23 @@ class Handle:
         check(lib.ccs_root_bounds(self._h, _ptr(states), len(states), _ptr(out)))
         return out
 
-    def solve(self, states: np.ndarray, opts: SolveOpts | None = None):
+    def solve(self, states: np.ndarray, opts: SolveOpts | None = None, table_ids=None):
+        """Solve packed states; ``table_ids`` (0 / 1 per cube) picks the first or the attached table."""
+
         states = np.ascontiguousarray(states, dtype=np.uint32).reshape(-1, 5)
         results = (Result * len(states))()
-        check(lib.ccs_solve(self._h, _ptr(states), len(states), ctypes.byref(opts or solve_opts()),
-                            ctypes.cast(results, ctypes.c_void_p)))
+        ids = None if table_ids is None else np.ascontiguousarray(table_ids, dtype=np.uint8).reshape(-1)
+        check(lib.ccs_solve_tables(self._h, _ptr(states), None if ids is None else _ptr(ids), len(states),
+                                   ctypes.byref(opts or solve_opts()), ctypes.cast(results, ctypes.c_void_p)))
         return list(results)
+
+    def attach_table(self, kind: str, fmt: str, path) -> None:
+        check(lib.ccs_attach_table(self._h, kind.encode(), FORMATS[fmt], str(path).encode()))
+
+    def probe_bench(self, n_states: int = 1 << 20, rounds: int = 256) -> tuple[float, float]:
+        rate, ms = ctypes.c_double(), ctypes.c_double()
+        check(lib.ccs_probe_bench(self._h, n_states, rounds, ctypes.byref(rate), ctypes.byref(ms)))
+        return rate.value, ms.value
 
     def last_solve_stats(self) -> tuple[float, int, int]:
         ms, probes, launches = ctypes.c_double(), ctypes.c_uint64(), ctypes.c_int()
@@ -242,10 +267,10 @@ class Handle:
     def server_start(self, slots: int, opts: SolveOpts | None = None) -> None:
         check(lib.ccs_server_start(self._h, slots, ctypes.byref(opts or solve_opts())))
 
-    def server_submit(self, state: np.ndarray) -> int:
+    def server_submit(self, state: np.ndarray, table_id: int = 0) -> int:
         state = np.ascontiguousarray(state, dtype=np.uint32).reshape(5)
         rid = ctypes.c_uint64()
-        check(lib.ccs_server_submit(self._h, _ptr(state), ctypes.byref(rid)))
+        check(lib.ccs_server_submit_table(self._h, _ptr(state), table_id, ctypes.byref(rid)))
         return rid.value
 
     def server_poll(self, max_out: int = 256):

@@ -16,6 +16,7 @@ import numpy as np
 from cuda_cube_solver import native
 from cuda_cube_solver.cubie import CubieState
 from cuda_cube_solver.device import state_words
+from cuda_cube_solver.solver import flipped_edges
 
 
 @dataclass
@@ -29,15 +30,20 @@ class Served:
 
 
 class Server:
-    """Continuous batching on one handle (its table must be loaded)."""
+    """Continuous batching on one handle (its table must be loaded).  ``flip_rule``: with a second
+    table attached, requests with at least this many flipped edges are searched with it."""
 
-    def __init__(self, handle: native.Handle, slots: int = 1024, opts: native.SolveOpts | None = None):
+    def __init__(self, handle: native.Handle, slots: int = 1024, opts: native.SolveOpts | None = None,
+                 flip_rule: int | None = None):
         self.h = handle
+        self.flip_rule = flip_rule
         self.h.server_start(slots, opts or native.solve_opts())
         self.submitted: dict[int, float] = {}
 
     def submit(self, state: CubieState) -> int:
-        rid = self.h.server_submit(state_words([state])[0])
+        words = state_words([state])
+        table = 0 if self.flip_rule is None else int(flipped_edges(words)[0] >= self.flip_rule)
+        rid = self.h.server_submit(words[0], table)
         self.submitted[rid] = time.perf_counter()
         return rid
 

@@ -145,21 +145,70 @@ class GpuSolver:
         self.last_kernel_ms = 0.0
         self.last_probes = 0
         self.variant = 0  # search kernel variant (libccs); 0 is the fastest measured
+        self.tuned: dict | None = None  # settings chosen by autotune(); else the cached ones
+        self.use_autotune = True
+        self.second_kind: str | None = None  # kind of the attached second table (table id 1)
+        self.flip_rule = FLIP_RULE
+
+    def attach_second(self, kind: str = "d4", path: Path | None = None, log=None) -> None:
+        """Keep a second table of ``kind`` resident beside the first (loaded from ``path``, else
+        built on the GPU).  Cubes with at least ``flip_rule`` flipped edges are then searched with it."""
+
+        if path is None:
+            self.handle.build_table(kind, self.table_format, None, keep_resident=2, log=log)
+        else:
+            self.handle.attach_table(kind, self.table_format, path)
+        self.second_kind = kind
+
+    def table_ids(self, words: np.ndarray) -> np.ndarray | None:
+        """Per cube 0 (first table) or 1 (second table, when attached) by the flip-count rule."""
+
+        if self.second_kind is None:
+            return None
+        return (flipped_edges(words) >= self.flip_rule).astype(np.uint8)
 
     @classmethod
-    def build_resident(cls, kind: str = "d4t", table_format: str = "block", log=None, device: int = 0, **kw):
-        """Build ``kind`` on the GPU and solve with it straight from device memory (no file)."""
+    def build_resident(cls, kind: str = "d4t", table_format: str = "block", log=None, device: int = 0,
+                       second_kind: str | None = None, **kw):
+        """Build ``kind`` on the GPU and solve with it straight from device memory (no file);
+        ``second_kind`` also builds a second resident table (see ``attach_second``)."""
 
         h = native.Handle(device)
         counts, secs = h.build_table(kind, table_format, None, keep_resident=True, log=log)
         solver = cls(kind=kind, table_format=table_format, handle=h, **kw)
         solver.build_counts, solver.build_seconds = counts, secs
+        if second_kind:
+            solver.attach_second(second_kind, log=log)
         return solver
 
-    def _opts(self, timeout_s: float = 0.0) -> native.SolveOpts:
+    def _opts(self, timeout_s: float = 0.0, n: int = 0) -> native.SolveOpts:
         blocks_per_sm = max(1, round(self.grid / self.sms)) if self.grid else 0
-        return native.solve_opts(self.prefix_len, self.deeper_prefix_at[:2], blocks_per_sm, 0, timeout_s,
-                                 variant=self.variant)
+        o = native.solve_opts(self.prefix_len, self.deeper_prefix_at[:2], blocks_per_sm, 0, timeout_s,
+                              variant=self.variant)
+        tuned = self.tuned if self.tuned is not None else None
+        if tuned is None and self.use_autotune:
+            from cuda_cube_solver import autotune
+
+            tuned = autotune.lookup(self.table_name, n or 1, self.handle.device)
+        if tuned:
+            o.variant, o.base_plen, o.spread = tuned["variant"], tuned["base_plen"], tuned["spread"]
+            o.move_min, o.move_age = tuned["move"]
+        return o
+
+    @property
+    def table_name(self) -> str:
+        return self.kind.name if self.table_format == "block" else f"{self.kind.name}-b3"
+
+    def autotune(self, sample: list[CubieState], log=None, save: bool = True) -> dict:
+        """Measure the kernel settings on ``sample`` and use the best from now on."""
+
+        from cuda_cube_solver import autotune
+
+        result = autotune.tune(self.handle, sample, self.table_name, log=log)
+        self.tuned = result["config"]
+        if save:
+            autotune.save(result, self.table_name, len(sample), self.handle.device)
+        return result
 
     def root_h(self, states: list[CubieState]) -> tuple[np.ndarray, np.ndarray]:
         words = state_words(states)
@@ -171,7 +220,7 @@ class GpuSolver:
             return []
         words = state_words(states)
         t0 = time.perf_counter()
-        results = self.handle.solve(words, self._opts())
+        results = self.handle.solve(words, self._opts(n=len(states)), self.table_ids(words))
         self.last_kernel_ms, self.last_probes, _ = self.handle.last_solve_stats()
         out = []
         for state, r in zip(states, results):
@@ -188,6 +237,19 @@ class GpuSolver:
 
     def close(self) -> None:
         self.handle.close()
+
+
+# Cubes with this many flipped edges or more go to the second table when one is attached: the
+# d4t table's E-content classes favour the few-flip cubes of uniform random scrambles, and d4 is
+# the faster table for highly flipped positions such as the superflip.
+FLIP_RULE = 10
+
+
+def flipped_edges(words: np.ndarray) -> np.ndarray:
+    """Number of flipped edges of each packed state (n, 5): bit 4 of the twelve edge bytes."""
+
+    b = np.ascontiguousarray(words, np.uint32).reshape(-1, 5).view(np.uint8).reshape(-1, 20)
+    return ((b[:, 8:] >> 4) & 1).sum(axis=1)
 
 
 def verify_solutions(words: np.ndarray, solutions: list[list[int]]) -> bool:

@@ -79,11 +79,17 @@ int ccs_load_table(ccs_handle* h, const char* kind, int format, const char* path
 /* Build a table on the device (table.generate + build_preset, table.py:82-129,170-200): exact
  * BFS, histogram self-check, encode in `format`.  If out_path is not NULL the solving file is
  * written there (through "<out_path>.tmp" and a rename).  If keep_resident, the solving table
- * stays loaded in the handle as if ccs_load_table had been called.  depth_counts receives up to
+ * stays loaded in the handle as if ccs_load_table had been called (keep_resident = 2: it becomes
+ * the second table, see ccs_attach_table).  depth_counts receives up to
  * max_depths per-depth entry counts, n_depths their number; seconds the build time (GPU work,
  * without the file write).  log may be NULL. */
 int ccs_build_table(ccs_handle* h, const char* kind, int format, const char* out_path, int keep_resident,
                     uint64_t* depth_counts, int max_depths, int* n_depths, double* seconds, ccs_log_fn log);
+
+/* A second resident table (table id 1) of the same kind family and format as the first, e.g. d4
+ * next to d4t: one search launch then serves cubes of either table, chosen per cube.  Loaded from
+ * a file here; ccs_build_table with keep_resident = 2 builds it in place instead. */
+int ccs_attach_table(ccs_handle* h, const char* kind, int format, const char* path);
 
 /* Copy the loaded solving table (n_bytes = its size) to host memory. */
 int ccs_table_bytes(ccs_handle* h, uint64_t* n_bytes);
@@ -132,8 +138,20 @@ typedef struct ccs_result {
  * every cube through its IDA* bounds on the device.  results[n]. */
 int ccs_solve(ccs_handle* h, const uint32_t* states, int n, const ccs_solve_opts* opts, ccs_result* results);
 
+/* ccs_solve with a table per cube: table_ids[n] of 0 (the first table) or 1 (the attached one). */
+int ccs_solve_tables(ccs_handle* h, const uint32_t* states, const uint8_t* table_ids, int n,
+                     const ccs_solve_opts* opts, ccs_result* results);
+
 /* Device time of the last ccs_solve's search kernels (ms) and its total table probes. */
 int ccs_last_solve_stats(ccs_handle* h, double* kernel_ms, uint64_t* probes, int* launches);
+
+/* Random 32-byte sector gather ceiling of a device (the table probes' memory roofline): random
+ * sector loads from a `bytes` buffer, 8 in flight per thread; sectors_per_s and the time. */
+int ccs_gather_bench(int device, uint64_t bytes, int rounds, double* sectors_per_s, double* ms);
+
+/* The probe step alone on the loaded table (random states: index + lower bound, no search
+ * control), for comparison with the search kernel's probe rate. */
+int ccs_probe_bench(ccs_handle* h, int n_states, int rounds, double* probes_per_s, double* ms);
 
 /* ---- server: continuous batching (thread-safe against each other) -------------------------
  * ccs_server_start runs a service thread that owns a persistent search launch over `slots`
@@ -142,6 +160,7 @@ int ccs_last_solve_stats(ccs_handle* h, double* kernel_ms, uint64_t* probes, int
  * the GPU are admitted into free slots without waiting for the running ones. */
 int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* opts);
 int ccs_server_submit(ccs_handle* h, const uint32_t* state, uint64_t* request_id);
+int ccs_server_submit_table(ccs_handle* h, const uint32_t* state, int table_id, uint64_t* request_id);
 int ccs_server_poll(ccs_handle* h, int max_out, uint64_t* request_ids, ccs_result* results, int* n_out);
 int ccs_server_stop(ccs_handle* h);
 
