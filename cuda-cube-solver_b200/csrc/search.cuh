@@ -28,7 +28,8 @@ struct alignas(16) Slot {
     unsigned long long iter_nodes[24];  // nodes per bound
     unsigned long long t_admit, t_done; // device globaltimer, ns
     uint32_t table;                  // 0: the handle's table, 1: its second resident table
-    uint32_t pad2[3];
+    uint32_t queued;                 // 1 while the work ring holds a live entry for this slot
+    uint32_t pad2[2];
 };
 
 struct QueueState {
@@ -67,6 +68,7 @@ struct SearchParams {
     uint32_t spread;                 // lanes take items from up to this many queued iterations
     uint32_t move_min;               // phased kernel: lanes waiting before a MOVE pass runs
     uint32_t move_age;               // phased kernel: iterations a waiting lane may be deferred
+    uint32_t probe_min;              // phased kernel: probe pass repeats while this many lanes probe
     unsigned long long* done_log;    // host-mapped completion log (server), may be null
     uint32_t done_log_cap;
 };

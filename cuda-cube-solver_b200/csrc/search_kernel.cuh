@@ -93,6 +93,18 @@ __device__ __forceinline__ void enqueue_slot(const SearchParams& P, uint32_t s) 
     atomicExch(&P.ring[pos % P.ring_cap], (lap << 32) | s);
 }
 
+// A slot has at most one live ring entry: it is queued only when it has none (the flag is cleared
+// by the lane that retires the entry, which then re-checks the ticket, so an iteration published
+// meanwhile is queued by one of the two).
+__device__ __forceinline__ void queue_slot(const SearchParams& P, uint32_t s) {
+    if (atomicExch(&P.slots[s].queued, 1u) == 0u) enqueue_slot(P, s);
+}
+
+__device__ __forceinline__ bool ticket_open(const SearchParams& P, unsigned long long tk) {
+    uint32_t i = (uint32_t)tk, pl = (uint32_t)(tk >> 56);
+    return pl <= (uint32_t)MAX_PLEN && i < P.n_prefix[pl];
+}
+
 __device__ __forceinline__ void publish_epoch(const SearchParams& P, uint32_t s, uint32_t plen, uint32_t bound,
                                               uint32_t epoch) {
     Slot& sl = P.slots[s];
@@ -100,7 +112,7 @@ __device__ __forceinline__ void publish_epoch(const SearchParams& P, uint32_t s,
     __threadfence();
     atomicExch(&sl.ticket, ticket_make(plen, bound, epoch));
     __threadfence();
-    enqueue_slot(P, s);
+    queue_slot(P, s);
 }
 
 __device__ __forceinline__ void finish_slot(const SearchParams& P, uint32_t s, uint32_t status) {
@@ -126,13 +138,53 @@ __device__ __forceinline__ void finish_slot(const SearchParams& P, uint32_t s, u
 // search, and other cubes fill the lanes), at most the bound.
 __device__ __forceinline__ uint32_t next_plen(const SearchParams& P, unsigned long long last_nodes, uint32_t bound) {
     uint32_t pl = P.base_plen + (last_nodes >= P.deeper_at[0]) + (last_nodes >= P.deeper_at[1]);
-    if (*(volatile uint32_t*)&P.q->active >= P.shallow_min_active)  // enough cubes to keep lanes busy
+    // cubes admitted and not finished (q->active also counts admissions being attempted, which
+    // briefly overshoots when many lanes race for the admission ring)
+    volatile QueueState* q = P.q;
+    const unsigned long long fin = q->finished;  // read first: then fin <= admitted
+    const unsigned long long in_flight = q->admit_head - fin;
+    if (in_flight >= P.shallow_min_active)  // enough cubes to keep lanes busy
         pl -= (uint32_t)(last_nodes < P.shallow_at[0]) + (uint32_t)(last_nodes < P.shallow_at[1]);
     pl = pl < 1u ? 1u : (pl > (uint32_t)MAX_PLEN ? (uint32_t)MAX_PLEN : pl);
     return pl < bound ? pl : bound;
 }
 
 enum FetchResult { FETCH_OK = 0, FETCH_EMPTY = 1, FETCH_FINISHED = 2, FETCH_ADMIT = 3 };
+
+// Keeps the ring's head moving so that the queued positions (tail - head) stay well under the
+// capacity: retired entries are passed, and once the ring is half full a live entry at the head
+// (a cube whose long iteration is still being handed out) is moved to the tail instead of holding
+// every later position behind it.  Entries are plain slot references, so a moved one serves the
+// same iteration from its new place.
+static __device__ __noinline__ void advance_head(const SearchParams& P) {
+    volatile QueueState* q = P.q;
+    for (int a = 0; a < 4; ++a) {
+        unsigned long long h = q->head, t = q->tail;
+        if (h >= t) return;
+        unsigned long long* cell = P.ring + h % P.ring_cap;
+        unsigned long long e = *(volatile unsigned long long*)cell;
+        unsigned long long lap = e >> 32, want = h / P.ring_cap;
+        if (lap < want || lap == 0xFFFFFFFFull) return;  // reserved by an enqueue, not yet written
+        if (lap == want && (uint32_t)e != RING_RETIRED) {
+            if (t - h < P.ring_cap / 2u) return;  // room left: the live entry stays
+            if (atomicCAS(cell, e, (e & 0xFFFFFFFF00000000ull) | RING_RETIRED) != e) return;
+            enqueue_slot(P, (uint32_t)e);
+        }
+        atomicCAS((unsigned long long*)&P.q->head, h, h + 1);  // retired, moved or overwritten
+    }
+}
+
+// Safety net run by an idle warp: queues any active cube whose current iteration still has items
+// to hand out but which has no ring entry (none should exist; the check is cheap).
+static __device__ __noinline__ void requeue_stranded(const SearchParams& P) {
+    for (uint32_t s = 0; s < P.n_slots; ++s) {
+        const Slot& sl = P.slots[s];
+        if (*(const volatile uint32_t*)&sl.status != SLOT_ACTIVE || *(const volatile uint32_t*)&sl.found ||
+            *(const volatile uint32_t*)&sl.queued)
+            continue;
+        if (ticket_open(P, *(const volatile unsigned long long*)&sl.ticket)) queue_slot(P, s);
+    }
+}
 
 // Next unit of work for a lane: a cube to admit (admission ring, first), or a prefix item of a
 // queued iteration (work ring).  FETCH_FINISHED when nothing is queued, admitted or in flight.
@@ -153,6 +205,7 @@ __device__ __forceinline__ int fetch_item(const SearchParams& P, uint32_t seed, 
             atomicSub(&P.q->active, 1u);
             continue;
         }
+        advance_head(P);
         unsigned long long h = q->head, t = q->tail;
         if (h >= t) return (q->active == 0u && q->admit_head >= q->admit_tail) ? FETCH_FINISHED : FETCH_EMPTY;
         // Lanes start at a seeded position among the first `spread` queued iterations and scan
@@ -177,7 +230,13 @@ __device__ __forceinline__ int fetch_item(const SearchParams& P, uint32_t seed, 
                         epoch = (uint32_t)(tk >> 32) & 0xFFFFu;
                         return FETCH_OK;
                     }
-                    atomicCAS(cell, e, (e & 0xFFFFFFFF00000000ull) | RING_RETIRED);  // iteration handed out
+                    // iteration handed out: retire the entry; if a new iteration was published
+                    // meanwhile (its queue_slot saw this entry still live), queue it now
+                    if (atomicCAS(cell, e, (e & 0xFFFFFFFF00000000ull) | RING_RETIRED) == e) {
+                        atomicExch(&P.slots[s].queued, 0u);
+                        __threadfence();
+                        if (ticket_open(P, *(volatile unsigned long long*)&P.slots[s].ticket)) queue_slot(P, s);
+                    }
                 }
                 if (pos == h) atomicCAS((unsigned long long*)&P.q->head, h, h + 1);
             }
@@ -447,6 +506,7 @@ f.load(sl.frame);
                 if (lane == 0) atomicOr(&P.q->error, ERR_IDLE_LIMIT);
                 break;
             }
+            if ((idle_polls & 1023u) == 64u && lane == 0) requeue_stranded(P);
             __nanosleep(backoff);
             backoff = backoff < 4096u ? backoff * 2u : 4096u;
             continue;

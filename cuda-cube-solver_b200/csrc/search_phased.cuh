@@ -184,24 +184,41 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                 if (lane == 0) atomicOr(&P.q->error, ERR_IDLE_LIMIT);
                 break;
             }
+            if ((idle_polls & 1023u) == 64u && lane == 0) requeue_stranded(P);
             __nanosleep(backoff);
             backoff = backoff < 4096u ? backoff * 2u : 4096u;
             continue;
         }
         idle_polls = 0;
         backoff = 32;
-        // PROBE frame k of child m.
-        if (eval) {
-            State t = f.get(k);
-            if (k < 3) move_right(T, t, T.frame_move[k][m]);
-            else move_left(T, t, T.inv_move[T.frame_move[k - 3][m]]);
-            uint32_t v = probe_bound<MODE, NEC, FMT>(T, P, t, second);
-            ++probes;
-            uint32_t parent = hget(h, k);
-            if (k < 3 && parent) v = max(v, parent - 1u);  // a right move changes the coset distance by <= 1
-            v = v > 31u ? 31u : v;
-            c = hset(c, k, v);
-            k = ((uint32_t)g + 1u + v > bound) ? 7 : next_frame(rem);
+        // PROBE frame k of child m.  A lane whose child is pruned takes its next sibling at once
+        // and the pass repeats while at least P.probe_min lanes have a probe; lanes that need the
+        // control phases (a child that passed every frame, a node without children left) wait
+        // for the pass to end.  Children are evaluated in the same order either way.
+        bool ev = eval;
+        for (;;) {
+            if (ev) {
+                State t = f.get(k);
+                if (k < 3) move_right(T, t, T.frame_move[k][m]);
+                else move_left(T, t, T.inv_move[T.frame_move[k - 3][m]]);
+                uint32_t v = probe_bound<MODE, NEC, FMT>(T, P, t, second);
+                ++probes;
+                uint32_t parent = hget(h, k);
+                if (k < 3 && parent) v = max(v, parent - 1u);  // a right move changes the coset distance by <= 1
+                v = v > 31u ? 31u : v;
+                c = hset(c, k, v);
+                k = ((uint32_t)g + 1u + v > bound) ? 7 : next_frame(rem);
+                if (k == 7 && todo != 0u) {  // pruned: the next sibling (PICK)
+                    m = __ffs(todo) - 1;
+                    todo &= todo - 1;
+                    ++nodes;
+                    c = h;
+                    rem = ord & ~(0x41041u << (3 + (m / 3) % 3));
+                    k = next_frame(rem);
+                }
+            }
+            ev = ev && k < 6;
+            if ((uint32_t)__popc(__ballot_sync(0xFFFFFFFFu, ev)) < P.probe_min) break;
         }
     }
 }

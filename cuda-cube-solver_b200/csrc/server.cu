@@ -176,6 +176,7 @@ extern "C" int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* 
     std::memset(s->done_log, 0, 8ull * s->log_cap);
     CCS_CUDA_TRY(cudaHostGetDevicePointer(&s->d_done_log, s->done_log, 0));
     fill_params(h, opts, &s->P);
+    s->P.n_slots = (uint32_t)slots;
     s->P.done_log = s->d_done_log;
     s->P.done_log_cap = s->log_cap;
     s->grid = grid_for(h, opts);

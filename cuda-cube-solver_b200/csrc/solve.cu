@@ -35,10 +35,11 @@ int ensure_search_buffers(ccs_handle* h, uint32_t slots) {
         h->slot_cap = 0;
         uint32_t cap = std::max<uint32_t>(slots, 64u);
         CCS_CUDA_TRY(cudaMalloc(&h->d_slots, sizeof(Slot) * cap));
-        // ring: each slot has at most one queued iteration; admission ring: one entry per slot
-        CCS_CUDA_TRY(cudaMalloc(&h->d_ring, sizeof(unsigned long long) * (3ull * cap + 64)));
+        // work ring: 4 positions per slot (its head is kept moving, see advance_head), then the
+        // admission ring: one entry per slot
+        CCS_CUDA_TRY(cudaMalloc(&h->d_ring, sizeof(unsigned long long) * (5ull * cap + 64)));
         h->slot_cap = cap;
-        h->ring_cap = 2 * cap + 64;
+        h->ring_cap = 4 * cap + 64;
     }
     return CCS_OK;
 }
@@ -71,6 +72,7 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
     P->spread = o && o->spread > 0 ? (uint32_t)o->spread : 4096u;
     P->move_min = o && o->move_min > 0 ? (uint32_t)o->move_min : 8u;
     P->move_age = o && o->move_age > 0 ? (uint32_t)o->move_age : 4u;
+    P->probe_min = o && o->probe_min > 0 ? (uint32_t)o->probe_min : 20u;
     P->done_log = nullptr;
     P->done_log_cap = 0;
 }
@@ -172,6 +174,7 @@ extern "C" int ccs_solve_tables(ccs_handle* h, const uint32_t* states, const uin
     q.admit_tail = (unsigned long long)n;
     SearchParams P;
     fill_params(h, opts, &P);
+    P.n_slots = (uint32_t)n;
     cudaStream_t st = h->stream;
     CCS_CUDA_TRY(cudaMemcpyAsync(h->d_slots, host.data(), sizeof(Slot) * n, cudaMemcpyHostToDevice, st));
     CCS_CUDA_TRY(cudaMemsetAsync(h->d_ring, 0xFF, sizeof(unsigned long long) * (h->ring_cap + h->slot_cap), st));

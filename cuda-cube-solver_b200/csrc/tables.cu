@@ -178,6 +178,7 @@ extern "C" int ccs_build_table(ccs_handle* h, const char* kind, int format, cons
                                ccs_log_fn log) {
     if (!h || !kind) return fail(CCS_E_ARG, "NULL argument");
     if (format != CCS_FMT_BLOCK && format != CCS_FMT_B3) return fail(CCS_E_ARG, "unknown table format %d", format);
+    const std::string first_kind = h->kind_name;  // restored after building a second table
     CCS_TRY(set_kind(h, kind));
     CCS_CUDA_TRY(cudaSetDevice(h->device));
     const KindDesc k = h->kind;
@@ -186,7 +187,6 @@ extern "C" int ccs_build_table(ccs_handle* h, const char* kind, int format, cons
     auto t0 = std::chrono::steady_clock::now();
 
     // keep_resident 1: the new table replaces the handle's tables; 2: it becomes the second table.
-    std::string first_kind = h->kind_name;
     if (keep_resident == 2 && !h->d_table) return fail(CCS_E_STATE, "no first table to attach a second one to");
     if (keep_resident == 1) free_table(h);
     DeviceBuffer<uint8_t> depth(n_chunks * 16);

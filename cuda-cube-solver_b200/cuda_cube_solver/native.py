@@ -48,6 +48,7 @@ class SolveOpts(ctypes.Structure):
         ("shallow_at1", ctypes.c_double),
         ("move_min", ctypes.c_int),
         ("move_age", ctypes.c_int),
+        ("probe_min", ctypes.c_int),
     ]
 
 
@@ -164,9 +165,10 @@ def gather_bench(device: int = 0, nbytes: int = 8 << 30, rounds: int = 64) -> tu
 
 def solve_opts(base_plen: int = 4, deeper_at: tuple[float, float] = (5e7, 3e9), blocks_per_sm: int = 0,
                threads: int = 0, timeout_s: float = 0.0, spread: int = 0, variant: int = 0,
-               shallow_at: tuple[float, float] = (0.0, 0.0), move_min: int = 0, move_age: int = 0) -> SolveOpts:
+               shallow_at: tuple[float, float] = (0.0, 0.0), move_min: int = 0, move_age: int = 0,
+               probe_min: int = 0) -> SolveOpts:
     return SolveOpts(base_plen, float(deeper_at[0]), float(deeper_at[1]), blocks_per_sm, threads, timeout_s, spread,
-                     variant, float(shallow_at[0]), float(shallow_at[1]), move_min, move_age)
+                     variant, float(shallow_at[0]), float(shallow_at[1]), move_min, move_age, probe_min)
 
 
 class Handle:

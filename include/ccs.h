@@ -122,6 +122,8 @@ typedef struct ccs_solve_opts {
     double shallow_at1;       /*   prefix one move shorter (0: 1e5 / 1.5e6, < 0: off)          */
     int move_min;             /* lanes waiting before a frame-update pass runs (0: 8)          */
     int move_age;             /* warp iterations a lane may wait for it (0: 4)                 */
+    int probe_min;            /* a warp keeps probing (pruned children -> next sibling) while  */
+                              /*   at least this many lanes have a probe (0: default, > 32: off) */
 } ccs_solve_opts;
 
 typedef struct ccs_result {
