@@ -88,6 +88,7 @@ _SIGS = {
     "ccs_lower_bound": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p],
     "ccs_root_bounds": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p],
     "ccs_solve": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _P(SolveOpts), ctypes.c_void_p],
+    "ccs_solve_noalloc": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _P(SolveOpts), ctypes.c_void_p],
     "ccs_solve_tables": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _P(SolveOpts), ctypes.c_void_p],
     "ccs_attach_table": [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p],
     "ccs_server_submit_table": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _P(ctypes.c_uint64)],
@@ -100,6 +101,7 @@ _SIGS = {
     "ccs_server_stop": [ctypes.c_void_p],
 }
 EXPORTED = tuple(_SIGS) + ("ccs_last_error",)
+NOALLOC_MAX_CUBES = 256  # CCS_NOALLOC_MAX_CUBES of ccs.h
 
 
 def _load():
@@ -250,6 +252,16 @@ class Handle:
         ids = None if table_ids is None else np.ascontiguousarray(table_ids, dtype=np.uint8).reshape(-1)
         check(lib.ccs_solve_tables(self._h, _ptr(states), None if ids is None else _ptr(ids), len(states),
                                    ctypes.byref(opts or solve_opts()), ctypes.cast(results, ctypes.c_void_p)))
+        return list(results)
+
+    def solve_noalloc(self, states: np.ndarray, opts: SolveOpts | None = None):
+        """``ccs_solve_noalloc``: the same search on the library's fixed buffers, for callers that
+        cannot allocate device memory at solve time (at most ``NOALLOC_MAX_CUBES`` cubes)."""
+
+        states = np.ascontiguousarray(states, dtype=np.uint32).reshape(-1, 5)
+        results = (Result * len(states))()
+        check(lib.ccs_solve_noalloc(self._h, _ptr(states), len(states), ctypes.byref(opts or solve_opts()),
+                                    ctypes.cast(results, ctypes.c_void_p)))
         return list(results)
 
     def attach_table(self, kind: str, fmt: str, path) -> None:

@@ -144,6 +144,19 @@ int ccs_solve(ccs_handle* h, const uint32_t* states, int n, const ccs_solve_opts
 int ccs_solve_tables(ccs_handle* h, const uint32_t* states, const uint8_t* table_ids, int n,
                      const ccs_solve_opts* opts, ccs_result* results);
 
+/* ccs_solve without any allocation, for callers that cannot allocate device memory while they
+ * solve: a process whose GPU memory is owned by a caching pool or a framework's allocator (its
+ * own cudaMalloc would fail or fragment the pool), or a service that fixes its memory footprint
+ * at start-up.  No counterpart in the reference.  The search buffers are one fixed array in the
+ * library's device image (304 KB on every GPU that loads the library); at most
+ * CCS_NOALLOC_MAX_CUBES cubes per call, prefixes of at most 4 moves (opts->base_plen <= 4;
+ * deeper_at0/1 are ignored), the first table only.  The first call on a device sets the array up
+ * (with that device current) and should come before any stream capture.  One array per process
+ * and device: calls that overlap on the GPU race on it. */
+#define CCS_NOALLOC_MAX_CUBES 256
+int ccs_solve_noalloc(ccs_handle* h, const uint32_t* states, int n, const ccs_solve_opts* opts,
+                      ccs_result* results);
+
 /* Device time of the last ccs_solve's search kernels (ms) and its total table probes. */
 int ccs_last_solve_stats(ccs_handle* h, double* kernel_ms, uint64_t* probes, int* launches);
 

@@ -54,3 +54,8 @@ def test_custom_group_kind_registration():
     assert np.array_equal(t["gen_class"], kinds.get("d4t").gen[0])
     with pytest.raises(native.CcsError, match="not normalised"):
         native.register_group_kind("swap01", [((1, 0, 2, 3), (0, 0, 0, 0))])
+
+
+def test_noalloc_limit_matches_header():
+    text = (ROOT / "include" / "ccs.h").read_text()
+    assert f"#define CCS_NOALLOC_MAX_CUBES {native.NOALLOC_MAX_CUBES}" in text
