@@ -191,7 +191,7 @@ def served_stream(args, solver, opts) -> dict:
             cubes.append(pool[ui])
             ui += 1
     arrivals = serving.poisson_arrivals(n, args.serve_rate, seed=3)
-    srv = serving.Server(solver.handle, 1024, opts)
+    srv = serving.Server(solver.handle, 1024, opts, flip_rule=solver.flip_rule if solver.second_kind else None)
     try:
         stats = serving.replay(srv, cubes, arrivals)
     finally:
@@ -203,7 +203,8 @@ def served_stream(args, solver, opts) -> dict:
     assert verify_solutions(state_words(cubes), [r.moves for r in results])
     stats.update({"mix": {"uniform": int((kinds_ == 0).sum()), "length_ge_18": int((kinds_ == 1).sum()),
                           "superflip": int((kinds_ == 2).sum())},
-                  "rate_per_s": args.serve_rate, "table": config_table(args)})
+                  "rate_per_s": args.serve_rate, "table": config_table(args),
+                  "second_table": solver.second_kind, "flip_rule": solver.flip_rule if solver.second_kind else None})
     return stats
 
 
@@ -262,7 +263,14 @@ def main() -> None:
     ap.add_argument("--serve", type=int, default=400, help="requests in the served-stream measurement (0: skip)")
     ap.add_argument("--tune", action="store_true", help="autotune the kernel settings on a separate sample first")
     ap.add_argument("--serve-rate", type=float, default=100.0, help="Poisson arrival rate of the served stream (/s)")
+    ap.add_argument("--second", default=None,
+                    help="second resident table for the served stream (default: d4 beside d4t; 'none' for none)")
+    ap.add_argument("--no-ceiling", action="store_true", help="skip the random-sector gather ceiling measurement")
     args = ap.parse_args()
+    if args.second is None:
+        args.second = "d4" if args.kind == "d4t" and args.format == "block" else ""
+    elif args.second == "none":
+        args.second = ""
 
     world, rank, local = dist_setup()
     from cuda_cube_solver import native, workloads
@@ -362,6 +370,8 @@ def main() -> None:
 
     served = None
     if args.serve:
+        if args.second:  # set-up: the second resident table for highly flipped requests
+            solver.attach_second(args.second)
         served = served_stream(args, solver, opts)
 
     peaks = measured_peaks()
@@ -373,6 +383,10 @@ def main() -> None:
                 "probes_per_cube": total_probes / (args.batch * args.steps),
                 "peak_source": "measured" if not peaks.get("fallback") else "fallback",
                 "note": "algorithmic bytes = 32-byte sector per table probe, counted on the device"}
+    if not args.no_ceiling:  # the random 32-byte sector gather ceiling of this GPU (untimed)
+        ceiling, _ = native.gather_bench(local, 8 << 30, 64)
+        roofline["random_sector_ceiling"] = {"sectors_per_s": ceiling, "gb_s": ceiling * SECTOR / 1e9,
+                                             "frac": roofline["probes_per_s"] / ceiling}
     traffic_file = ROOT / "profiles" / "search_traffic.json"
     if traffic_file.exists():
         tr = json.loads(traffic_file.read_text())
@@ -393,7 +407,7 @@ def main() -> None:
                    "d2h_bytes_per_step": native.ctypes.sizeof(native.Result) * args.batch},
            "gpu_launches": int(sum(launches)),
            "kernel_settings": {"variant": opts.variant, "base_plen": opts.base_plen, "spread": opts.spread,
-                               "move_min": opts.move_min, "move_age": opts.move_age,
+                               "move_min": opts.move_min, "move_age": opts.move_age, "probe_min": opts.probe_min,
                                "autotuned": tuned is not None},
            "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
            "plain": plain, "served": served, "table_build_s": build_s, "table_build_gpu_s": solver.build_seconds,

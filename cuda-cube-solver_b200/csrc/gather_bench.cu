@@ -38,7 +38,7 @@ __global__ void __launch_bounds__(256) k_gather(const uint32_t* __restrict__ buf
             load_sector(buf + s * 8u, w[l]);
         }
 #pragma unroll
-        for (int l = 0; l < LANES; ++l) acc += w[l][0] ^ w[l][(x[l] >> 13) & 7];
+        for (int l = 0; l < LANES; ++l) acc += w[l][0] ^ pick8(w[l], (uint32_t)(x[l] >> 13) & 7u);
     }
     if (acc == 0x12345678u) atomicAdd(sink, 1ull);  // keeps the loads alive
 }
@@ -68,7 +68,25 @@ __global__ void __launch_bounds__(256) k_probe_only(const DevTables* __restrict_
 
 }  // namespace
 
+// The ceiling is the best of a few launch shapes (independent loads in flight per thread x
+// resident blocks per SM), so that it does not understate what the memory system delivers.
+template <int LANES>
+static int time_gather(const uint32_t* buf, uint64_t n_sectors, int grid, int rounds, unsigned long long* sink,
+                       cudaEvent_t a, cudaEvent_t b, double* rate, float* t_ms) {
+    k_gather<LANES><<<grid, 256>>>(buf, n_sectors, 2, sink);  // warm-up
+    CCS_CUDA_TRY(cudaEventRecord(a));
+    k_gather<LANES><<<grid, 256>>>(buf, n_sectors, rounds, sink);
+    CCS_CUDA_TRY(cudaEventRecord(b));
+    CCS_CUDA_TRY(cudaEventSynchronize(b));
+    float t = 0;
+    CCS_CUDA_TRY(cudaEventElapsedTime(&t, a, b));
+    *rate = (double)grid * 256.0 * LANES * rounds / (t * 1e-3);
+    *t_ms = t;
+    return CCS_OK;
+}
+
 extern "C" int ccs_gather_bench(int device, uint64_t bytes, int rounds, double* sectors_per_s, double* ms) {
+    if (rounds <= 0 || bytes < 32) return fail(CCS_E_ARG, "bad arguments");
     CCS_CUDA_TRY(cudaSetDevice(device));
     int sms = 0;
     CCS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
@@ -77,21 +95,26 @@ extern "C" int ccs_gather_bench(int device, uint64_t bytes, int rounds, double* 
     if (!buf.ok() || !sink.ok()) return fail(CCS_E_NOMEM, "gather buffer of %llu bytes", (unsigned long long)bytes);
     CCS_CUDA_TRY(cudaMemset(buf.p, 0x5A, bytes));
     const uint64_t n_sectors = bytes / 32;
-    const int grid = sms * 8;
     cudaEvent_t a, b;
     CCS_CUDA_TRY(cudaEventCreate(&a));
     CCS_CUDA_TRY(cudaEventCreate(&b));
-    k_gather<8><<<grid, 256>>>(buf.p, n_sectors, 4, sink.p);  // warm-up
-    CCS_CUDA_TRY(cudaEventRecord(a));
-    k_gather<8><<<grid, 256>>>(buf.p, n_sectors, rounds, sink.p);
-    CCS_CUDA_TRY(cudaEventRecord(b));
-    CCS_CUDA_TRY(cudaEventSynchronize(b));
-    float t = 0;
-    CCS_CUDA_TRY(cudaEventElapsedTime(&t, a, b));
+    double best = 0, rate = 0;
+    float best_ms = 0, t = 0;
+    int rc = CCS_OK;
+    for (int bps : {4, 8}) {
+        const int grid = sms * bps;
+        if (rc == CCS_OK) rc = time_gather<4>(buf.p, n_sectors, grid, rounds * 2, sink.p, a, b, &rate, &t);
+        if (rc == CCS_OK && rate > best) best = rate, best_ms = t;
+        if (rc == CCS_OK) rc = time_gather<8>(buf.p, n_sectors, grid, rounds, sink.p, a, b, &rate, &t);
+        if (rc == CCS_OK && rate > best) best = rate, best_ms = t;
+        if (rc == CCS_OK) rc = time_gather<16>(buf.p, n_sectors, grid, (rounds + 1) / 2, sink.p, a, b, &rate, &t);
+        if (rc == CCS_OK && rate > best) best = rate, best_ms = t;
+    }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    if (ms) *ms = t;
-    if (sectors_per_s) *sectors_per_s = (double)grid * 256.0 * 8.0 * rounds / (t * 1e-3);
+    if (rc != CCS_OK) return rc;
+    if (ms) *ms = best_ms;
+    if (sectors_per_s) *sectors_per_s = best;
     return CCS_OK;
 }
 

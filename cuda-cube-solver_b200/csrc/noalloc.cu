@@ -27,7 +27,8 @@ using namespace ccs;
 
 namespace ccs {
 void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P);
-int grid_for(ccs_handle* h, const ccs_solve_opts* o);
+int resolve_variant(const ccs_solve_opts* o, int cubes);
+int grid_for(ccs_handle* h, const ccs_solve_opts* o, int variant);
 int launch_kernel(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream, int variant);
 void make_slot(const uint32_t state[5], uint32_t request, uint32_t table, Slot* s);
 void fill_result(const Slot& s, ccs_result* r);
@@ -154,7 +155,8 @@ extern "C" int ccs_solve_noalloc(ccs_handle* h, const uint32_t* states, int n, c
     CCS_CUDA_TRY(cudaMemcpyAsync(P.admit, g_host_admit, 8ull * n, cudaMemcpyHostToDevice, st));
     CCS_CUDA_TRY(cudaMemcpyAsync(&S->q, &q, sizeof q, cudaMemcpyHostToDevice, st));
 
-    const int grid = grid_for(h, opts);
+    const int variant = resolve_variant(opts, n);
+    const int grid = grid_for(h, opts, variant);
     const double timeout = opts && opts->timeout_s > 0 ? opts->timeout_s : 0;
     auto t0 = std::chrono::steady_clock::now();
     double kernel_ms = 0;
@@ -162,7 +164,7 @@ extern "C" int ccs_solve_noalloc(ccs_handle* h, const uint32_t* states, int n, c
     unsigned long long prev_probes = ~0ull;
     for (;;) {
         CCS_CUDA_TRY(cudaEventRecord(h->ev0, st));
-        CCS_TRY(launch_kernel(h, P, grid, st, opts ? opts->variant : 0));
+        CCS_TRY(launch_kernel(h, P, grid, st, variant));
         CCS_CUDA_TRY(cudaEventRecord(h->ev1, st));
         CCS_CUDA_TRY(cudaMemcpyAsync(&q, &S->q, sizeof q, cudaMemcpyDeviceToHost, st));
         CCS_CUDA_TRY(cudaStreamSynchronize(st));

@@ -16,7 +16,7 @@
 
 namespace ccs {
 
-template <int MODE, int NEC, int FMT, int THREADS, int MINB>
+template <int MODE, int NEC, int FMT, int THREADS, int MINB, bool LOOKAHEAD = false>
 __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevTables* __restrict__ gT, SearchParams P) {
     __shared__ DevTables T;
     extern __shared__ uint32_t frame_smem[];
@@ -36,6 +36,9 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
     const uint32_t lane_seed = (blockIdx.x * blockDim.x + threadIdx.x) * 0x9E3779B1u >> 7;
 
     int mv = 0;  // frame update this lane waits for: 0 none, 1 push child m, 2 pop one level
+    // LOOKAHEAD: the next sibling of the child under evaluation, evaluated alongside it
+    int m2 = -1, k2 = 7;
+    uint32_t c2 = 0, rem2 = 0;
     uint32_t move_age = 0;
     for (;;) {
         // RESOLVE the child under evaluation: drop a pruned one, test a leaf survivor for a
@@ -111,6 +114,7 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
             todo = 0u;
             g = 0;
             m = -1;
+            m2 = -1;
         }
         // FINISH the item; the lane finishing an iteration's last item closes the iteration.
         if (have && mv == 0 && m < 0 && todo == 0u && g == 0) {
@@ -197,7 +201,56 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
         // for the pass to end.  Children are evaluated in the same order either way.
         bool ev = eval;
         for (;;) {
-            if (ev) {
+            if (ev && LOOKAHEAD) {
+                // The child's next frame and the next sibling's next frame are probed together
+                // (two independent load chains in flight).  Results are taken in DFS order: the
+                // sibling becomes the current child when this one is pruned; if this one passes
+                // every frame, the sibling goes back to `todo` (its probes so far are repeated
+                // after the subtree).
+                if (m2 >= 0 && k2 == 7) m2 = -1;  // the sibling was pruned: it is done
+                if (m2 < 0 && todo != 0u) {
+                    m2 = __ffs(todo) - 1;
+                    todo &= todo - 1;
+                    ++nodes;
+                    c2 = h;
+                    rem2 = ord & ~(0x41041u << (3 + (m2 / 3) % 3));
+                    k2 = next_frame(rem2);
+                }
+                const bool two = m2 >= 0 && k2 < 6;
+                const int kb = two ? k2 : k, mb = two ? m2 : m;
+                State t = f.get(k), u = f.get(kb);
+                frame_do(T, t, k, m);
+                frame_do(T, u, kb, mb);
+                const uint64_t i1 = table_index_dev<MODE, NEC>(T, P.classidx, t, second);
+                const uint64_t i2 = table_index_dev<MODE, NEC>(T, P.classidx, u, second);
+                const uint32_t* tab = second ? P.table2 : P.table;
+                uint32_t v = lower_bound_dev<FMT>(tab, i1), w = lower_bound_dev<FMT>(tab, i2);
+                probes += two ? 2u : 1u;
+                uint32_t parent = hget(h, k);
+                if (k < 3 && parent) v = max(v, parent - 1u);
+                v = v > 31u ? 31u : v;
+                c = hset(c, k, v);
+                k = ((uint32_t)g + 1u + v > bound) ? 7 : next_frame(rem);
+                if (two) {
+                    parent = hget(h, kb);
+                    if (kb < 3 && parent) w = max(w, parent - 1u);
+                    w = w > 31u ? 31u : w;
+                    c2 = hset(c2, kb, w);
+                    k2 = ((uint32_t)g + 1u + w > bound) ? 7 : next_frame(rem2);
+                }
+                if (k == 7 && m2 >= 0) {  // pruned: the sibling takes over
+                    m = m2;
+                    c = c2;
+                    rem = rem2;
+                    k = k2;
+                    m2 = -1;
+                }
+                if (k == 6 && m2 >= 0) {  // passed every frame: the sibling waits for the subtree
+                    todo |= 1u << m2;
+                    --nodes;
+                    m2 = -1;
+                }
+            } else if (ev) {
                 State t = f.get(k);
                 if (k < 3) move_right(T, t, T.frame_move[k][m]);
                 else move_left(T, t, T.inv_move[T.frame_move[k - 3][m]]);
@@ -208,6 +261,8 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                 v = v > 31u ? 31u : v;
                 c = hset(c, k, v);
                 k = ((uint32_t)g + 1u + v > bound) ? 7 : next_frame(rem);
+            }
+            if (ev) {
                 if (k == 7 && todo != 0u) {  // pruned: the next sibling (PICK)
                     m = __ffs(todo) - 1;
                     todo &= todo - 1;

@@ -23,7 +23,8 @@ using namespace ccs;
 
 namespace ccs {
 void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P);
-int grid_for(ccs_handle* h, const ccs_solve_opts* o);
+int resolve_variant(const ccs_solve_opts* o, int cubes);
+int grid_for(ccs_handle* h, const ccs_solve_opts* o, int variant);
 int launch_kernel(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream, int variant);
 void make_slot(const uint32_t state[5], uint32_t request, uint32_t table, Slot* s);
 void fill_result(const Slot& s, ccs_result* r);
@@ -37,6 +38,7 @@ struct Server {
     bool kernel_running = false;
     SearchParams P{};
     int grid = 0;
+    int variant = 2;  // resolved kernel variant (automatic: sibling lookahead, for latency)
     unsigned long long* done_log = nullptr;  // host-mapped
     unsigned long long* d_done_log = nullptr;
     uint32_t log_cap = 0;
@@ -109,7 +111,7 @@ int Server::step() {
     // 3. keep a search launch running while cubes are in flight
     if (kernel_running && cudaEventQuery(kernel_done) == cudaSuccess) kernel_running = false;
     if (!kernel_running && in_flight > 0) {
-        CCS_TRY(launch_kernel(h, P, grid, h->stream, opts.variant));
+        CCS_TRY(launch_kernel(h, P, grid, h->stream, variant));
         CCS_CUDA_TRY(cudaEventRecord(kernel_done, h->stream));
         kernel_running = true;
     }
@@ -179,7 +181,8 @@ extern "C" int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* 
     s->P.n_slots = (uint32_t)slots;
     s->P.done_log = s->d_done_log;
     s->P.done_log_cap = s->log_cap;
-    s->grid = grid_for(h, opts);
+    s->variant = resolve_variant(opts, 0);
+    s->grid = grid_for(h, opts, s->variant);
     QueueState q;
     std::memset(&q, 0, sizeof q);
     CCS_CUDA_TRY(cudaMemsetAsync(h->d_ring, 0xFF, sizeof(unsigned long long) * (h->ring_cap + h->slot_cap), s->copy));

@@ -72,21 +72,28 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
     P->spread = o && o->spread > 0 ? (uint32_t)o->spread : 4096u;
     P->move_min = o && o->move_min > 0 ? (uint32_t)o->move_min : 8u;
     P->move_age = o && o->move_age > 0 ? (uint32_t)o->move_age : 4u;
-    P->probe_min = o && o->probe_min > 0 ? (uint32_t)o->probe_min : 20u;
+    P->probe_min = o && o->probe_min > 0 ? (uint32_t)o->probe_min : 16u;
     P->done_log = nullptr;
     P->done_log_cap = 0;
 }
 
-int grid_for(ccs_handle* h, const ccs_solve_opts* o) {
-    int variant = o ? o->variant : 0;
-    int bps = o && o->blocks_per_sm > 0 ? o->blocks_per_sm : (variant == 0 ? 3 : 2);
+// Kernel variants (ccs_solve_opts.variant): 1 = phase-ordered control, frames in shared memory,
+// 256 threads x 2 blocks per SM (registers for every value, no spills; the throughput kernel);
+// 2 = the same with sibling lookahead (two probe chains per lane: lower latency when few cubes
+// are searched, more probes); 3 = phase-ordered, 256 x 3 (80 registers); 4 = loop control,
+// frames in registers, 256 x 2; 5 = loop control, frames in shared memory, 512 x 2.
+// 0 = automatic: 2 for fewer than 64 cubes (and for the server), else 1.
+int resolve_variant(const ccs_solve_opts* o, int cubes) {
+    int v = o ? o->variant : 0;
+    if (v <= 0 || v > 5) v = cubes < 64 ? 2 : 1;
+    return v;
+}
+
+int grid_for(ccs_handle* h, const ccs_solve_opts* o, int variant) {
+    int bps = o && o->blocks_per_sm > 0 ? o->blocks_per_sm : (variant == 3 ? 3 : 2);
     return bps * h->sms;
 }
 
-// Launch shapes: 0 (default) = phase-ordered control, frames in shared memory, 256 threads, 3
-// blocks per SM (24 warps, 64 registers); 1 = the same with 512 threads, 2 blocks per SM; 2 = loop
-// control, frames in registers, 256 threads, 2 blocks per SM; 3 = loop control, frames in shared
-// memory, 512 threads.
 template <int MODE, int NEC, int FMT, int THREADS, bool SMEM, int MINB>
 int launch_variant(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream) {
     auto* k = search_kernel<MODE, NEC, FMT, THREADS, SMEM, MINB>;
@@ -97,9 +104,9 @@ int launch_variant(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t 
     return CCS_OK;
 }
 
-template <int MODE, int NEC, int FMT, int THREADS, int MINB>
+template <int MODE, int NEC, int FMT, int THREADS, int MINB, bool LOOKAHEAD = false>
 int launch_phased(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream) {
-    auto* k = search_kernel_phased<MODE, NEC, FMT, THREADS, MINB>;
+    auto* k = search_kernel_phased<MODE, NEC, FMT, THREADS, MINB, LOOKAHEAD>;
     constexpr size_t dyn = search_dyn_smem<true, THREADS>();
     if (dyn) CCS_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
     k<<<grid, THREADS, dyn, stream>>>(h->d_tables, P);
@@ -107,14 +114,16 @@ int launch_phased(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t s
     return CCS_OK;
 }
 
+// variant: a resolved one (1..5).
 int launch_kernel(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream, int variant) {
     return dispatch_kind(h->kind, [&](auto M, auto N) {
         return dispatch_fmt(h->format, [&](auto F) {
             constexpr int MODE = decltype(M)::value, NEC = decltype(N)::value, FMT = decltype(F)::value;
-            if (variant == 1) return launch_phased<MODE, NEC, FMT, 512, 2>(h, P, grid, stream);
-            if (variant == 2) return launch_variant<MODE, NEC, FMT, SEARCH_THREADS, false, 1>(h, P, grid, stream);
-            if (variant == 3) return launch_variant<MODE, NEC, FMT, 512, true, 2>(h, P, grid, stream);
-            return launch_phased<MODE, NEC, FMT, 256, 3>(h, P, grid, stream);
+            if (variant == 2) return launch_phased<MODE, NEC, FMT, 256, 2, true>(h, P, grid, stream);
+            if (variant == 3) return launch_phased<MODE, NEC, FMT, 256, 3>(h, P, grid, stream);
+            if (variant == 4) return launch_variant<MODE, NEC, FMT, SEARCH_THREADS, false, 2>(h, P, grid, stream);
+            if (variant == 5) return launch_variant<MODE, NEC, FMT, 512, true, 2>(h, P, grid, stream);
+            return launch_phased<MODE, NEC, FMT, 256, 2>(h, P, grid, stream);
         });
     });
 }
@@ -181,7 +190,8 @@ extern "C" int ccs_solve_tables(ccs_handle* h, const uint32_t* states, const uin
     CCS_CUDA_TRY(cudaMemcpyAsync(P.admit, admit.data(), 8ull * n, cudaMemcpyHostToDevice, st));
     CCS_CUDA_TRY(cudaMemcpyAsync(h->d_q, &q, sizeof q, cudaMemcpyHostToDevice, st));
 
-    const int grid = grid_for(h, opts);
+    const int variant = resolve_variant(opts, n);
+    const int grid = grid_for(h, opts, variant);
     const double timeout = opts && opts->timeout_s > 0 ? opts->timeout_s : 0;
     auto t0 = std::chrono::steady_clock::now();
     double kernel_ms = 0;
@@ -189,7 +199,7 @@ extern "C" int ccs_solve_tables(ccs_handle* h, const uint32_t* states, const uin
     unsigned long long prev_probes = ~0ull;
     for (;;) {
         CCS_CUDA_TRY(cudaEventRecord(h->ev0, st));
-        CCS_TRY(launch_kernel(h, P, grid, st, opts ? opts->variant : 0));
+        CCS_TRY(launch_kernel(h, P, grid, st, variant));
         CCS_CUDA_TRY(cudaEventRecord(h->ev1, st));
         CCS_CUDA_TRY(cudaMemcpyAsync(&q, h->d_q, sizeof q, cudaMemcpyDeviceToHost, st));
         CCS_CUDA_TRY(cudaStreamSynchronize(st));

@@ -3,7 +3,9 @@ GPU, table and batch size by measuring them.
 
 Knobs (``native.SolveOpts``):
 
-* ``variant``: block shape -- 0 = 256 threads x 3 blocks per SM (24 warps), 1 = 512 x 2 (32 warps);
+* ``variant``: search kernel -- 1 = throughput (256 threads x 2 blocks per SM), 2 = sibling
+  lookahead (two probe chains per lane: lower latency for few cubes), 3 = 256 x 3 blocks per SM;
+  0 = the library's automatic choice;
 * ``base_plen``: cut depth of the work items (prefix length of a cube's iterations);
 * ``move_min`` / ``move_age``: how many lanes wait, and for how many iterations, before the
   frame-update pass (push / pop) runs -- the depth of the lanes' update pipeline;
@@ -27,17 +29,19 @@ from cuda_cube_solver.device import state_words
 CACHE = Path(os.environ.get("CCS_TUNE_CACHE", Path.home() / ".cache" / "cuda_cube_solver" / "autotune.json"))
 
 SPACE = {
-    "variant": [0, 1],
+    "variant": [1, 2, 3],
     "base_plen": [3, 4, 5],
     "move": [(4, 2), (8, 4), (12, 6), (16, 8)],
     "spread": [512, 1024, 4096],
+    "probe_min": [12, 16, 20, 24],
 }
-DEFAULT = {"variant": 0, "base_plen": 4, "move": (8, 4), "spread": 4096}
+DEFAULT = {"variant": 0, "base_plen": 4, "move": (8, 4), "spread": 4096, "probe_min": 16}
 
 
 def opts_of(cfg: dict, timeout_s: float = 600.0) -> native.SolveOpts:
     return native.solve_opts(base_plen=cfg["base_plen"], variant=cfg["variant"], spread=cfg["spread"],
-                             move_min=cfg["move"][0], move_age=cfg["move"][1], timeout_s=timeout_s)
+                             move_min=cfg["move"][0], move_age=cfg["move"][1], timeout_s=timeout_s,
+                             probe_min=cfg.get("probe_min", 0))
 
 
 def batch_bucket(n: int) -> str:

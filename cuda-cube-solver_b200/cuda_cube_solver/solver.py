@@ -144,7 +144,7 @@ class GpuSolver:
         self.block = block
         self.last_kernel_ms = 0.0
         self.last_probes = 0
-        self.variant = 0  # search kernel variant (libccs); 0 is the fastest measured
+        self.variant = 0  # search kernel variant (libccs); 0 lets the library choose by batch size
         self.tuned: dict | None = None  # settings chosen by autotune(); else the cached ones
         self.use_autotune = True
         self.second_kind: str | None = None  # kind of the attached second table (table id 1)
@@ -193,6 +193,7 @@ class GpuSolver:
         if tuned:
             o.variant, o.base_plen, o.spread = tuned["variant"], tuned["base_plen"], tuned["spread"]
             o.move_min, o.move_age = tuned["move"]
+            o.probe_min = tuned.get("probe_min", 0)
         return o
 
     @property
@@ -239,10 +240,11 @@ class GpuSolver:
         self.handle.close()
 
 
-# Cubes with this many flipped edges or more go to the second table when one is attached: the
-# d4t table's E-content classes favour the few-flip cubes of uniform random scrambles, and d4 is
-# the faster table for highly flipped positions such as the superflip.
-FLIP_RULE = 10
+# Cubes with this many flipped edges or more go to the second table when one is attached.  Measured
+# on one B200 with d4t and d4 resident: the superflip (all 12 edges flipped) takes 13.5 G probes on
+# d4 against 72.7 G on d4t (5.1x faster), while uniform cubes with 10 flipped edges are still
+# faster on d4t (127 vs 103 cubes/s), so only fully flipped positions switch.
+FLIP_RULE = 12
 
 
 def flipped_edges(words: np.ndarray) -> np.ndarray:

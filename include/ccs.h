@@ -117,7 +117,8 @@ typedef struct ccs_solve_opts {
     int threads;              /* threads per block: 128, 256 or 512 (0: default)            */
     double timeout_s;         /* give up after this long (0: no limit)                      */
     int spread;               /* lanes work on up to this many queued cubes at once (0: 4096) */
-    int variant;              /* search kernel variant (see solve.cu); 0: default                */
+    int variant;              /* search kernel: 0 automatic, 1 throughput, 2 sibling lookahead */
+                              /*   (latency), 3-5 other launch shapes (see solve.cu)            */
     double shallow_at0;       /* an iteration of < this many nodes makes the next one use a    */
     double shallow_at1;       /*   prefix one move shorter (0: 1e5 / 1.5e6, < 0: off)          */
     int move_min;             /* lanes waiting before a frame-update pass runs (0: 8)          */

@@ -34,3 +34,14 @@ def test_poisson_arrivals():
     t = serving.poisson_arrivals(20000, 100.0, seed=3)
     assert np.all(np.diff(t) > 0)
     assert abs(len(t) / t[-1] - 100.0) < 3.0
+
+
+def test_flipped_edges_and_the_table_rule():
+    from cuda_cube_solver.device import state_words
+    from cuda_cube_solver.solver import FLIP_RULE, flipped_edges
+
+    cubes = [CubieState(), workloads.superflip()] + workloads.uniform_cubes(64, seed=5)
+    n = flipped_edges(state_words(cubes))
+    assert n[0] == 0 and n[1] == 12
+    assert all(x % 2 == 0 for x in n)  # edge flips have even parity
+    assert (n >= FLIP_RULE).sum() >= 1 and FLIP_RULE == 12
