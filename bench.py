@@ -208,6 +208,22 @@ def served_stream(args, solver, opts) -> dict:
     return stats
 
 
+def build_report(args, solver, peaks) -> dict:
+    """The table build of the set-up (GPU BFS + encoding): entries per second and the
+    algorithmic DRAM write bandwidth (one depth byte per entry, then the encoded table)."""
+
+    from cuda_cube_solver import native
+
+    nec, entries = native.kind_info(args.kind)
+    table_bytes = solver.handle.table_bytes()
+    secs = solver.build_seconds
+    written = entries + table_bytes
+    return {"kind": args.kind, "format": args.format, "gpu_seconds": secs, "entries": entries,
+            "entries_per_s": entries / secs, "table_bytes": table_bytes,
+            "write_gb_s": written / secs / 1e9, "write_frac_of_hbm": written / secs / 1e9 / float(peaks["hbm_gbs"]),
+            "depth_counts": solver.build_counts}
+
+
 def config_table(args) -> str:
     return args.kind if args.format == "block" else f"{args.kind}-b3"
 
@@ -257,7 +273,7 @@ def main() -> None:
     ap.add_argument("--impl", default="mine", choices=["mine", "reference", "reference-gpu"])
     ap.add_argument("--ref-batch", type=int, default=100, help="reference-gpu: cubes per solve call (its CLI default)")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
-    ap.add_argument("--plain", type=int, default=32, help="cubes solved one per call for the plain numbers")
+    ap.add_argument("--plain", type=int, default=200, help="cubes solved one per call for the plain numbers")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--variant", type=int, default=0, help="search kernel variant (libccs ccs_solve_opts.variant)")
     ap.add_argument("--serve", type=int, default=400, help="requests in the served-stream measurement (0: skip)")
@@ -356,17 +372,21 @@ def main() -> None:
         barrier(world)
         return
 
-    # ---- plain: one cube per call (the drop-in path), per-cube latency ----
-    plain_lat = []
-    for s in my_states[: args.plain]:
+    # ---- plain: one cube per call (the drop-in path), per-cube latency: uniform cubes of seed 1 ----
+    plain_lat, plain_probes, plain_dev = [], 0, 0.0
+    for s in workloads.uniform_cubes(args.plain, seed=1):
         t0 = time.perf_counter()
         solver.solve([s])
         plain_lat.append(time.perf_counter() - t0)
+        plain_probes += solver.last_probes
+        plain_dev += solver.last_kernel_ms / 1000.0
     plain = None
     if plain_lat:
-        plain = {"cubes": len(plain_lat), "cubes_per_s": len(plain_lat) / sum(plain_lat),
+        plain = {"cubes": len(plain_lat), "workload": "uniform random cubes (seed 1), one per call",
+                 "cubes_per_s": len(plain_lat) / sum(plain_lat),
                  "p50_s": float(np.percentile(plain_lat, 50)), "p99_s": float(np.percentile(plain_lat, 99)),
-                 "worst_s": max(plain_lat)}
+                 "worst_s": max(plain_lat), "probes_per_s": plain_probes / plain_dev if plain_dev else None,
+                 "batched_over_plain": value / (len(plain_lat) / sum(plain_lat))}
 
     served = None
     if args.serve:
@@ -411,6 +431,7 @@ def main() -> None:
                                "autotuned": tuned is not None},
            "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
            "plain": plain, "served": served, "table_build_s": build_s, "table_build_gpu_s": solver.build_seconds,
+           "table_build": build_report(args, solver, peaks),
            "wall_s_per_step": statistics.mean(wall)}
     print(json.dumps(out))
     barrier(world)

@@ -42,11 +42,23 @@ __device__ __forceinline__ uint32_t labels8(uint32_t v) { return ((v & 0x0303030
 // Byte-wise values < 8 as a prmt selector (nibble j = byte j).
 __device__ __forceinline__ uint32_t nib_sel(uint32_t v) { return prmt(v | (v >> 4), 0u, 0x4420u); }
 
+// Corner words of s * m (the corner half of move_right).
+__device__ __forceinline__ void corners_right(const DevTables& T, uint32_t& c0, uint32_t& c1, int m) {
+    uint32_t a = prmt(c0, c1, T.mv_csel[m][0]) + T.mv_cadd[m][0];
+    uint32_t b = prmt(c0, c1, T.mv_csel[m][1]) + T.mv_cadd[m][1];
+    c0 = wrap_twist(a);
+    c1 = wrap_twist(b);
+}
+
+// Corner words of m * s (the corner half of move_left).
+__device__ __forceinline__ void corners_left(const DevTables& T, uint32_t& c0, uint32_t& c1, int m) {
+    const uint32_t l0 = T.lf_c[m][0], l1 = T.lf_c[m][1];
+    c0 = wrap_twist(prmt(l0, l1, nib_sel(c0 & 0x07070707u)) + (c0 & 0x18181818u));
+    c1 = wrap_twist(prmt(l0, l1, nib_sel(c1 & 0x07070707u)) + (c1 & 0x18181818u));
+}
+
 __device__ __forceinline__ void move_right(const DevTables& T, State& s, int m) {
-    uint32_t a = prmt(s.c0, s.c1, T.mv_csel[m][0]) + T.mv_cadd[m][0];
-    uint32_t b = prmt(s.c0, s.c1, T.mv_csel[m][1]) + T.mv_cadd[m][1];
-    s.c0 = wrap_twist(a);
-    s.c1 = wrap_twist(b);
+    corners_right(T, s.c0, s.c1, m);
     uint32_t o[3];
 #pragma unroll
     for (int w = 0; w < 3; ++w) {
@@ -62,9 +74,7 @@ __device__ __forceinline__ void move_right(const DevTables& T, State& s, int m) 
 
 // s <- m * s: every cubie c (and its orientation) is renamed through the move.
 __device__ __forceinline__ void move_left(const DevTables& T, State& s, int m) {
-    const uint32_t l0 = T.lf_c[m][0], l1 = T.lf_c[m][1];
-    s.c0 = wrap_twist(prmt(l0, l1, nib_sel(s.c0 & 0x07070707u)) + (s.c0 & 0x18181818u));
-    s.c1 = wrap_twist(prmt(l0, l1, nib_sel(s.c1 & 0x07070707u)) + (s.c1 & 0x18181818u));
+    corners_left(T, s.c0, s.c1, m);
     const uint32_t r0 = T.lf_e[m][0], r1 = T.lf_e[m][1], r2 = T.lf_e[m][2];
     uint32_t e[3] = {s.e0, s.e1, s.e2};
 #pragma unroll
@@ -79,12 +89,16 @@ __device__ __forceinline__ void move_left(const DevTables& T, State& s, int m) {
     s.e2 = e[2];
 }
 
-__device__ __forceinline__ uint32_t corner_raw_dev(const DevTables& T, const State& s) {
-    uint32_t olo = (s.c0 >> 3) & 0x03030303u;
-    uint32_t ohi = (s.c1 >> 3) & 0x00030303u;
+__device__ __forceinline__ uint32_t corner_raw_words(const DevTables& T, uint32_t c0, uint32_t c1) {
+    uint32_t olo = (c0 >> 3) & 0x03030303u;
+    uint32_t ohi = (c1 >> 3) & 0x00030303u;
     uint32_t twist = __dp4a(olo, 0x1B090301u, 0u) + 81u * __dp4a(ohi, 0x00090301u, 0u);
-    uint32_t dmask = gather4(s.c0, 2) | (gather4(s.c1, 2) << 4);
+    uint32_t dmask = gather4(c0, 2) | (gather4(c1, 2) << 4);
     return twist * 70u + T.ccomb_rank[dmask];
+}
+
+__device__ __forceinline__ uint32_t corner_raw_dev(const DevTables& T, const State& s) {
+    return corner_raw_words(T, s.c0, s.c1);
 }
 
 // Edge coordinate of M_sym g M_sym^-1, computed without conjugating the cubie labels: a U-D
@@ -129,6 +143,9 @@ struct KindTraits {
     static constexpr uint64_t N_EDGE = MODE == KIND_304 ? 495ull * 70ull * 16ull : 495ull * 256ull * (uint64_t)NEC;
 };
 
+// Table formats.
+enum Format : int { FMT_BLOCK = 0, FMT_B3 = 1 };
+
 // second: index into the second resident table's kind (genc2).
 template <int MODE, int NEC>
 __device__ __forceinline__ uint64_t table_index_dev(const DevTables& T, const uint32_t* __restrict__ classidx,
@@ -137,8 +154,7 @@ __device__ __forceinline__ uint64_t table_index_dev(const DevTables& T, const ui
     return (uint64_t)(packed >> 4) * KindTraits<MODE, NEC>::N_EDGE + edge_coord_sym<MODE, NEC>(T, s, packed & 15u, second);
 }
 
-// Table formats.
-enum Format : int { FMT_BLOCK = 0, FMT_B3 = 1 };
+
 
 // The whole 32-byte sector of a probe in one 256-bit load: one sector request instead of two
 // (the minimum and the offset word travel separately otherwise).  The table is read-only while
@@ -161,16 +177,12 @@ __device__ __forceinline__ uint32_t pick8(const uint32_t w[8], uint32_t i) {
     return r;
 }
 
-// Lower bound of entry idx.  Block: per 32-byte sector a u8 minimum then 124 two-bit offsets
-// (3 = at least minimum + 3) starting at bit 8.  Base 3: header m | cut << 6, then 155 digits,
-// five per byte (digit 0 = at least m, 1 = m + cut + 1, 2 = at least m + cut + 2).
+// Value of entry j of a loaded sector.  Block: a u8 minimum then 124 two-bit offsets (3 = at
+// least minimum + 3) starting at bit 8.  Base 3: header m | cut << 6, then 155 digits, five per
+// byte (digit 0 = at least m, 1 = m + cut + 1, 2 = at least m + cut + 2).
 template <int FMT>
-__device__ __forceinline__ uint32_t lower_bound_dev(const uint32_t* __restrict__ tab, uint64_t idx) {
-    uint32_t w[8];
+__device__ __forceinline__ uint32_t decode_sector(const uint32_t w[8], uint32_t j) {
     if (FMT == FMT_B3) {
-        uint64_t b = idx / 155u;
-        uint32_t j = (uint32_t)(idx - b * 155u);
-        load_sector(tab + b * 8u, w);
         uint32_t q = 1u + j / 5u;
         uint32_t hdr = w[0] & 0xFFu, byte = (pick8(w, q >> 2) >> (8u * (q & 3u))) & 0xFFu;
         uint32_t k = j % 5u;
@@ -179,11 +191,56 @@ __device__ __forceinline__ uint32_t lower_bound_dev(const uint32_t* __restrict__
         uint32_t m = hdr & 63u;
         return d == 0u ? m : m + (hdr >> 6) + d;
     } else {
-        uint64_t b = idx / 124u;
-        uint32_t pos = 8u + 2u * (uint32_t)(idx - b * 124u);
-        load_sector(tab + b * 8u, w);
+        uint32_t pos = 8u + 2u * j;
         return (w[0] & 0xFFu) + ((pick8(w, pos >> 5) >> (pos & 31u)) & 3u);
     }
+}
+
+template <int FMT>
+struct SectorTraits {
+    static constexpr uint32_t PER = FMT == FMT_B3 ? 155u : 124u;  // entries per 32-byte sector
+};
+
+// Lower bound of entry idx.
+template <int FMT>
+__device__ __forceinline__ uint32_t lower_bound_dev(const uint32_t* __restrict__ tab, uint64_t idx) {
+    constexpr uint32_t PER = SectorTraits<FMT>::PER;
+    uint32_t w[8];
+    uint64_t b = idx / PER;
+    load_sector(tab + b * 8u, w);
+    return decode_sector<FMT>(w, (uint32_t)(idx - b * PER));
+}
+
+// Lower bound of entry cls * NE + e (NE edge coordinates per corner class) in 32-bit arithmetic:
+// cls * NE = cls * (NE / PER) * PER + cls * (NE % PER), and every term fits 32 bits for the
+// kinds built here (at most 9,930 classes, 3,041,280 edge coordinates, 2^32 sectors).
+template <int FMT, uint64_t NE>
+__device__ __forceinline__ void split_sector(uint32_t cls, uint32_t e, uint32_t& sector, uint32_t& j) {
+    constexpr uint32_t PER = SectorTraits<FMT>::PER;
+    constexpr uint32_t Q = (uint32_t)(NE / PER), R = (uint32_t)(NE % PER);
+    static_assert(NE / PER * 9930ull < (1ull << 32) && R * 9930ull + NE < (1ull << 32), "32-bit sector arithmetic");
+    const uint32_t t = cls * R + e;
+    const uint32_t tq = t / PER;
+    sector = cls * Q + tq;
+    j = t - tq * PER;
+}
+
+template <int FMT, uint64_t NE>
+__device__ __forceinline__ uint32_t lower_bound_split(const uint32_t* __restrict__ tab, uint32_t cls, uint32_t e) {
+    uint32_t sector, j, w[8];
+    split_sector<FMT, NE>(cls, e, sector, j);
+    load_sector(tab + (uint64_t)sector * 8u, w);
+    return decode_sector<FMT>(w, j);
+}
+
+// One probe of the search: the lower bound of state s, the same value as
+// lower_bound_dev(tab, table_index_dev(T, classidx, s, second)) with 32-bit sector arithmetic.
+template <int MODE, int NEC, int FMT>
+__device__ __forceinline__ uint32_t probe_dev(const DevTables& T, const uint32_t* __restrict__ classidx,
+                                              const uint32_t* __restrict__ tab, const State& s, bool second = false) {
+    uint32_t packed = __ldg(classidx + corner_raw_dev(T, s));
+    return lower_bound_split<FMT, KindTraits<MODE, NEC>::N_EDGE>(tab, packed >> 4,
+                                                                 edge_coord_sym<MODE, NEC>(T, s, packed & 15u, second));
 }
 
 __device__ __forceinline__ bool is_solved(const State& s) {

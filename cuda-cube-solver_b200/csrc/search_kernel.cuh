@@ -249,7 +249,7 @@ __device__ __forceinline__ int fetch_item(const SearchParams& P, uint32_t seed, 
 template <int MODE, int NEC, int FMT>
 __device__ __forceinline__ uint32_t probe_bound(const DevTables& T, const SearchParams& P, const State& s,
                                                 bool second = false) {
-    return lower_bound_dev<FMT>(second ? P.table2 : P.table, table_index_dev<MODE, NEC>(T, P.classidx, s, second));
+    return probe_dev<MODE, NEC, FMT>(T, P.classidx, second ? P.table2 : P.table, s, second);
 }
 
 // Admission of a new cube: root bounds of its six frames, first threshold, first iteration.

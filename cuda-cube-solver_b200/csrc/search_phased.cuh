@@ -36,9 +36,12 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
     const uint32_t lane_seed = (blockIdx.x * blockDim.x + threadIdx.x) * 0x9E3779B1u >> 7;
 
     int mv = 0;  // frame update this lane waits for: 0 none, 1 push child m, 2 pop one level
-    // LOOKAHEAD: the next sibling of the child under evaluation, evaluated alongside it
+    // LOOKAHEAD: the next sibling of the child under evaluation, evaluated alongside it; when the
+    // child is pushed, the sibling's partial evaluation waits in a per-level stash (bit g of
+    // `stash`) and becomes the current child when the subtree pops back to level g.
     int m2 = -1, k2 = 7;
-    uint32_t c2 = 0, rem2 = 0;
+    uint32_t c2 = 0, rem2 = 0, stash = 0;
+    uint32_t la_c[LOOKAHEAD ? MAX_DEPTH : 1], la_x[LOOKAHEAD ? MAX_DEPTH : 1];
     uint32_t move_age = 0;
     for (;;) {
         // RESOLVE the child under evaluation: drop a pruned one, test a leaf survivor for a
@@ -59,6 +62,13 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                 }
             }
             if (mv == 0) m = -1;
+            if (LOOKAHEAD && mv == 0 && m2 >= 0) {  // the child is done: its sibling takes over
+                m = m2;
+                c = c2;
+                rem = rem2;
+                k = k2;
+                m2 = -1;
+            }
         }
         // A node with no children left pops one level.
         if (have && m < 0 && todo == 0u && g > 0 && mv == 0) mv = 2;
@@ -85,6 +95,12 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                         f.put(j, t);
                     }
                     if (mv == 1) {
+                        if (LOOKAHEAD && m2 >= 0 && k2 != 7) {  // (a pruned sibling is done)
+                            la_c[g] = c2;
+                            la_x[g] = rem2 | ((uint32_t)m2 << 18) | ((uint32_t)k2 << 23);
+                            stash |= 1u << g;
+                        }
+                        m2 = -1;
                         hstack[g] = h;
                         path[g] = (unsigned char)m;
                         h = c;
@@ -103,6 +119,15 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                                    ~((2u << mm) - 1u);
                             ord = frame_order(h, bound - (uint32_t)g);
                         }
+                        if (LOOKAHEAD && ((stash >> g) & 1u)) {  // the stashed sibling resumes
+                            stash &= ~(1u << g);
+                            const uint32_t x = la_x[g];
+                            c = la_c[g];
+                            rem = x & 0x3FFFFu;
+                            m = (int)((x >> 18) & 31u);
+                            k = (int)((x >> 23) & 7u);
+                            todo &= ~((2u << m) - 1u);
+                        }
                     }
                     mv = 0;
                 }
@@ -115,6 +140,7 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
             g = 0;
             m = -1;
             m2 = -1;
+            stash = 0u;
         }
         // FINISH the item; the lane finishing an iteration's last item closes the iteration.
         if (have && mv == 0 && m < 0 && todo == 0u && g == 0) {
@@ -163,6 +189,8 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                     g = 0;
                     nodes = 0;
                     probes = 0;
+                    stash = 0u;
+                    m2 = -1;
                     uint32_t allow = plen ? 1u << (pseq & 31u) : T.amask[0];
                     todo = allow & ~axis_move_mask(excluded_axes(h, bound));
                     ord = frame_order(h, bound);
@@ -204,9 +232,8 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
             if (ev && LOOKAHEAD) {
                 // The child's next frame and the next sibling's next frame are probed together
                 // (two independent load chains in flight).  Results are taken in DFS order: the
-                // sibling becomes the current child when this one is pruned; if this one passes
-                // every frame, the sibling goes back to `todo` (its probes so far are repeated
-                // after the subtree).
+                // sibling becomes the current child when this one is pruned or resolved, and waits
+                // in the stash while this one's subtree is searched.
                 if (m2 >= 0 && k2 == 7) m2 = -1;  // the sibling was pruned: it is done
                 if (m2 < 0 && todo != 0u) {
                     m2 = __ffs(todo) - 1;
@@ -221,10 +248,9 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                 State t = f.get(k), u = f.get(kb);
                 frame_do(T, t, k, m);
                 frame_do(T, u, kb, mb);
-                const uint64_t i1 = table_index_dev<MODE, NEC>(T, P.classidx, t, second);
-                const uint64_t i2 = table_index_dev<MODE, NEC>(T, P.classidx, u, second);
                 const uint32_t* tab = second ? P.table2 : P.table;
-                uint32_t v = lower_bound_dev<FMT>(tab, i1), w = lower_bound_dev<FMT>(tab, i2);
+                uint32_t v = probe_dev<MODE, NEC, FMT>(T, P.classidx, tab, t, second);
+                uint32_t w = probe_dev<MODE, NEC, FMT>(T, P.classidx, tab, u, second);
                 probes += two ? 2u : 1u;
                 uint32_t parent = hget(h, k);
                 if (k < 3 && parent) v = max(v, parent - 1u);
@@ -243,11 +269,6 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                     c = c2;
                     rem = rem2;
                     k = k2;
-                    m2 = -1;
-                }
-                if (k == 6 && m2 >= 0) {  // passed every frame: the sibling waits for the subtree
-                    todo |= 1u << m2;
-                    --nodes;
                     m2 = -1;
                 }
             } else if (ev) {

@@ -105,6 +105,23 @@ int emul_unrank(const char* name, const uint64_t* idx, int n, uint32_t* out_w) {
     });
 }
 
+// Sector and entry of cls * NE + e by the search's 32-bit arithmetic (split_sector).
+int emul_split_sector(const char* name, int fmt, const uint32_t* cls, const uint32_t* e, int n, uint64_t* out) {
+    Kind* k = kind(name);
+    if (!k) return -1;
+    return with_kind(k->desc, [&](auto M, auto N) {
+        constexpr uint64_t NE = KindTraits<decltype(M)::value, decltype(N)::value>::N_EDGE;
+        for (int i = 0; i < n; ++i) {
+            uint32_t sector, j;
+            if (fmt) split_sector<FMT_B3, NE>(cls[i], e[i], sector, j);
+            else split_sector<FMT_BLOCK, NE>(cls[i], e[i], sector, j);
+            out[2 * i] = sector;
+            out[2 * i + 1] = j;
+        }
+        return 0;
+    });
+}
+
 int emul_lower_bound(const uint32_t* table, int fmt, const uint64_t* idx, int n, uint32_t* out) {
     for (int i = 0; i < n; ++i) out[i] = fmt ? lower_bound_dev<FMT_B3>(table, idx[i]) : lower_bound_dev<FMT_BLOCK>(table, idx[i]);
     return 0;

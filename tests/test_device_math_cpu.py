@@ -12,6 +12,7 @@ import pytest
 
 from conftest import ROOT
 from cuda_cube_solver.cubie import MOVES_HTM, CubieState, compose
+from cuda_cube_solver import native
 from cuda_cube_solver.device import state_words
 
 KINDS = ["304", "s4", "d4f", "a4t", "d4t", "d4", "a4"]
@@ -95,3 +96,24 @@ def test_device_decoders_match_oracle(emul, oracle):
                 m, cut = int(sec[0]) & 63, int(sec[0]) >> 6
                 want.append(m if d == 0 else m + cut + d)
         assert out.tolist() == want
+
+
+@pytest.mark.parametrize("name", ["304", "s4", "d4f", "a4t", "d4t", "d4", "a4"])
+@pytest.mark.parametrize("fmt", [0, 1])
+def test_search_sector_arithmetic_matches_64_bit_division(emul, name, fmt):
+    """The search computes the sector of entry cls * NE + e in 32-bit arithmetic; it must equal
+    the 64-bit quotient and remainder by the entries per sector, edge cases included."""
+
+    nec, entries = native.kind_info(name)
+    ne = entries // 9930
+    rng = np.random.default_rng(7)
+    cls = np.concatenate([[0, 0, 9929, 9929, 1, 4965], rng.integers(0, 9930, 4000)]).astype(np.uint32)
+    e = np.concatenate([[0, ne - 1, 0, ne - 1, ne - 1, ne // 2], rng.integers(0, ne, 4000)]).astype(np.uint32)
+    out = np.zeros((len(cls), 2), np.uint64)
+    emul.emul_split_sector.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                       ctypes.c_void_p]
+    assert emul.emul_split_sector(name.encode(), fmt, cls.ctypes.data, e.ctypes.data, len(cls), out.ctypes.data) == 0
+    per = 155 if fmt else 124
+    idx = cls.astype(np.uint64) * np.uint64(ne) + e.astype(np.uint64)
+    assert np.array_equal(out[:, 0], idx // np.uint64(per))
+    assert np.array_equal(out[:, 1], idx % np.uint64(per))
