@@ -201,7 +201,18 @@ def served_stream(args, solver, opts) -> dict:
     from cuda_cube_solver.device import state_words
 
     assert verify_solutions(state_words(cubes), [r.moves for r in results])
-    stats.update({"mix": {"uniform": int((kinds_ == 0).sum()), "length_ge_18": int((kinds_ == 1).sum()),
+    # the same cubes in one batched solve (untimed): every served length must equal it
+    batched = [len(sol.moves) for sol in solver.solve(cubes)]
+    lat = np.array([r.latency_s for r in results])
+    per_kind = {}
+    for code, name in ((0, "uniform"), (1, "length_ge_18"), (2, "superflip")):
+        sel = lat[kinds_ == code]
+        if len(sel):
+            per_kind[name] = {"p50_s": float(np.percentile(sel, 50)), "p95_s": float(np.percentile(sel, 95)),
+                              "max_s": float(sel.max())}
+    stats.update({"lengths_equal_to_batched": [r.length for r in results] == batched, "latency_by_kind": per_kind,
+                  "slots": 1024, "search_state_bytes": 1024 * (416 + 5 * 8),
+                  "mix": {"uniform": int((kinds_ == 0).sum()), "length_ge_18": int((kinds_ == 1).sum()),
                           "superflip": int((kinds_ == 2).sum())},
                   "rate_per_s": args.serve_rate, "table": config_table(args),
                   "second_table": solver.second_kind, "flip_rule": solver.flip_rule if solver.second_kind else None})
