@@ -63,6 +63,23 @@ def test_s4_b3_counts_and_bytes(depth_golden):
         h.close()
 
 
+@pytest.mark.parametrize("preset", ["s4-b3", "d4f-b3", "a4t-b3", "a4t", "d4t-b3", "a4-b3", "a4", "d4-b3"])
+def test_every_preset_is_byte_identical_to_the_reference(preset):
+    """Each remaining preset built here has the sha256 of the table the reference's own kernels
+    build on a B200 (the 304, d4t and d4 tables are checked above)."""
+
+    p = kinds.PRESET_BY_NAME[preset]
+    ref = _ref_sha()[preset]
+    h = native.Handle()
+    try:
+        counts, _ = h.build_table(p.kind, p.format, None, keep_resident=True)
+        assert counts == ref["reference_counts"]
+        assert h.table_bytes() == p.table_bytes == ref["bytes"]
+        assert _sha(h.table_copy()) == ref["reference_sha256"]
+    finally:
+        h.close()
+
+
 def test_file_roundtrip_and_size_check(tmp_path):
     h = resident_handle("304")
     path = tmp_path / "prune-ud-304-blk.bin"
