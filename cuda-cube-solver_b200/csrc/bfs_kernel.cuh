@@ -102,44 +102,72 @@ __global__ void __launch_bounds__(256) bfs_forward(const DevTables* __restrict__
     add_count(P.counter, local);
 }
 
-// Backward pass: an unvisited entry with a neighbour at depth d is at depth d + 1.
+// Backward pass: an unvisited entry with a neighbour at depth d is at depth d + 1.  A warp takes
+// 32 consecutive 16-entry chunks (512 entries), lists their unvisited entries in shared memory,
+// and its lanes take the listed entries in turn, so the work is shared evenly however the
+// unvisited entries fall.  An entry tries its 18 neighbours one face at a time (three turns:
+// three independent table reads in flight) and stops at the first face with a neighbour at depth
+// d.  Lanes write single bytes: an entry's byte is only ever written by the lane that took it,
+// and readers only test for depth d, which no write of this pass produces or removes.
 template <int MODE, int NEC>
 __global__ void __launch_bounds__(256) bfs_backward(const DevTables* __restrict__ gT, BfsParams P, uint32_t d) {
     __shared__ DevTables T;
+    __shared__ uint16_t list[8][512];
     stage_tables(T, gT);
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     unsigned long long local = 0;
-    uint4* chunks = reinterpret_cast<uint4*>(P.depth);
-    for (uint64_t ch = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; ch < P.n_chunks;
-         ch += (uint64_t)gridDim.x * blockDim.x) {
-        uint4 v = chunks[ch];
-        uint32_t w[4] = {v.x, v.y, v.z, v.w};
-        bool changed = false;
+    const uint4* chunks = reinterpret_cast<const uint4*>(P.depth);
+    const uint8_t* depth = P.depth;
+    const uint64_t n_groups = (P.n_chunks + 31u) / 32u;
+    const uint64_t n_warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    for (uint64_t gi = blockIdx.x * (uint64_t)(blockDim.x >> 5) + warp; gi < n_groups; gi += n_warps) {
+        const uint64_t ch = gi * 32u + lane;
+        uint32_t unvisited = 0;  // bit j: entry j of this lane's chunk is unvisited
+        if (ch < P.n_chunks) {
+            uint4 v = chunks[ch];
+            uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            uint32_t x = w[q];
-            uint32_t hit = x & (x << 1) & (x << 2) & (x << 3) & (x << 4) & (x << 5) & (x << 6) & (x << 7) &
-                           0x80808080u;  // 0x80 where byte == 0xFF
-            while (hit) {
-                uint32_t b = (__ffs(hit) - 1) >> 3;
-                hit &= hit - 1;
-                uint64_t idx = ch * 16u + (uint64_t)q * 4u + b;
-                if (idx >= P.n_entries) break;
-                State s;
-                unrank_dev<MODE, NEC>(T, P.class_rep, idx, s);
-                for (int m = 0; m < 18; ++m) {
-                    State n = s;
-                    move_right(T, n, m);
-                    uint64_t j = table_index_dev<MODE, NEC>(T, P.classidx, n);
-                    if (((volatile uint8_t*)P.depth)[j] == d) {
-                        w[q] = (w[q] & ~(0xFFu << (8 * b))) | ((d + 1u) << (8 * b));
-                        changed = true;
-                        ++local;
-                        break;
-                    }
-                }
+            for (int q = 0; q < 4; ++q) {
+                uint32_t x = w[q];
+                uint32_t hit = x & (x << 1) & (x << 2) & (x << 3) & (x << 4) & (x << 5) & (x << 6) & (x << 7) &
+                               0x80808080u;  // 0x80 where byte == 0xFF
+                unvisited |= ((((hit >> 7) & 0x01010101u) * 0x01020408u) >> 24) << (4 * q);
             }
         }
-        if (changed) chunks[ch] = make_uint4(w[0], w[1], w[2], w[3]);
+        const uint32_t cnt = __popc(unvisited);
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= (uint32_t)o) incl += t;
+        }
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        uint32_t pos = incl - cnt;
+        for (uint32_t mm = unvisited; mm; mm &= mm - 1) list[warp][pos++] = (uint16_t)(lane * 16u + (__ffs(mm) - 1));
+        __syncwarp();
+        for (uint32_t it = lane; it < total; it += 32u) {
+            const uint64_t idx = gi * 512u + list[warp][it];
+            if (idx >= P.n_entries) continue;
+            State s;
+            unrank_dev<MODE, NEC>(T, P.class_rep, idx, s);
+            bool found = false;
+            for (int f = 0; f < 6 && !found; ++f) {
+                State n0 = s, n1 = s, n2 = s;
+                move_right(T, n0, 3 * f);
+                move_right(T, n1, 3 * f + 1);
+                move_right(T, n2, 3 * f + 2);
+                const uint64_t j0 = table_index_dev<MODE, NEC>(T, P.classidx, n0);
+                const uint64_t j1 = table_index_dev<MODE, NEC>(T, P.classidx, n1);
+                const uint64_t j2 = table_index_dev<MODE, NEC>(T, P.classidx, n2);
+                const uint32_t b0 = depth[j0], b1 = depth[j1], b2 = depth[j2];
+                found = b0 == d || b1 == d || b2 == d;
+            }
+            if (found) {
+                P.depth[idx] = (uint8_t)(d + 1u);
+                ++local;
+            }
+        }
+        __syncwarp();
     }
     add_count(P.counter, local);
 }
