@@ -69,35 +69,94 @@ __global__ void bfs_seed(const DevTables* __restrict__ gT, BfsParams P) {
     atomicAdd(P.counter, (unsigned long long)claim_with_stabilizer<MODE, NEC>(T, P, s, 0u));
 }
 
-// Forward pass: expand every entry at depth d.
+// Lists, in shared memory, the entries of a warp's 32 consecutive 16-entry chunks whose depth
+// byte equals `match` (as offsets 0..511 from the group's first entry); returns how many.
+__device__ __forceinline__ uint32_t list_group(const BfsParams& P, uint64_t gi, uint32_t lane, uint32_t match,
+                                               uint16_t* list) {
+    const uint64_t ch = gi * 32u + lane;
+    uint32_t sel = 0;  // bit j: entry j of this lane's chunk matches
+    if (ch < P.n_chunks) {
+        const uint4 v = reinterpret_cast<const uint4*>(P.depth)[ch];
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint32_t x = w[q] ^ (match * 0x01010101u);
+            const uint32_t hit = ~(((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x | 0x7F7F7F7Fu);  // 0x80 where byte == match
+            sel |= ((((hit >> 7) & 0x01010101u) * 0x01020408u) >> 24) << (4 * q);
+        }
+    }
+    const uint32_t cnt = __popc(sel);
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= (uint32_t)o) incl += t;
+    }
+    uint32_t pos = incl - cnt;
+    for (uint32_t mm = sel; mm; mm &= mm - 1) list[pos++] = (uint16_t)(lane * 16u + (__ffs(mm) - 1));
+    __syncwarp();
+    return __shfl_sync(0xFFFFFFFFu, incl, 31);
+}
+
+// Forward pass: expand every entry at depth d.  A warp lists the depth-d entries of 512
+// consecutive entries and its lanes take them in turn; an entry's 18 neighbours are claimed one
+// face at a time (three class lookups, then three depth tests in flight), each with its
+// stabiliser images.
 template <int MODE, int NEC>
 __global__ void __launch_bounds__(256) bfs_forward(const DevTables* __restrict__ gT, BfsParams P, uint32_t d) {
     __shared__ DevTables T;
+    __shared__ uint16_t list[8][512];
     stage_tables(T, gT);
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     unsigned long long local = 0;
-    const uint4* chunks = reinterpret_cast<const uint4*>(P.depth);
-    for (uint64_t ch = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; ch < P.n_chunks;
-         ch += (uint64_t)gridDim.x * blockDim.x) {
-        uint4 v = chunks[ch];
-        uint32_t w[4] = {v.x, v.y, v.z, v.w};
+    const uint8_t* depth = P.depth;
+    const uint32_t d1 = d + 1u;
+    const uint64_t n_groups = (P.n_chunks + 31u) / 32u;
+    const uint64_t n_warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    for (uint64_t gi = blockIdx.x * (uint64_t)(blockDim.x >> 5) + warp; gi < n_groups; gi += n_warps) {
+        const uint32_t total = list_group(P, gi, lane, d, list[warp]);
+        for (uint32_t it = lane; it < total; it += 32u) {
+            const uint64_t idx = gi * 512u + list[warp][it];
+            if (idx >= P.n_entries) continue;
+            State s;
+            unrank_dev<MODE, NEC>(T, P.class_rep, idx, s);
+            for (int f = 0; f < 6; ++f) {
+                State n[3];
+                uint32_t packed[3], stab[3];
+                uint64_t j[3];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            uint32_t x = w[q] ^ (d * 0x01010101u);
-            uint32_t hit = ~(((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x | 0x7F7F7F7Fu);  // 0x80 where byte == d
-            while (hit) {
-                uint32_t b = (__ffs(hit) - 1) >> 3;
-                hit &= hit - 1;
-                uint64_t idx = ch * 16u + (uint64_t)q * 4u + b;
-                if (idx >= P.n_entries) break;
-                State s;
-                unrank_dev<MODE, NEC>(T, P.class_rep, idx, s);
-                for (int m = 0; m < 18; ++m) {
-                    State n = s;
-                    move_right(T, n, m);
-                    local += claim_with_stabilizer<MODE, NEC>(T, P, n, d + 1u);
+                for (int i = 0; i < 3; ++i) {
+                    n[i] = s;
+                    move_right(T, n[i], 3 * f + i);
+                    packed[i] = __ldg(P.classidx + corner_raw_dev(T, n[i]));
+                }
+#pragma unroll
+                for (int i = 0; i < 3; ++i) stab[i] = __ldg(P.class_stab + (packed[i] >> 4));
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const uint32_t t = stab[i] ? __ffs(stab[i]) - 1 : 0u;
+                    j[i] = (uint64_t)(packed[i] >> 4) * KindTraits<MODE, NEC>::N_EDGE +
+                           edge_coord_sym<MODE, NEC>(T, n[i], T.sym_mul[t][packed[i] & 15u]);
+                }
+                uint32_t b[3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) b[i] = depth[j[i]];  // a stale 0xFF is settled by the atomic
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    if (stab[i] && b[i] == 0xFFu) local += claim_entry(P.depth, j[i], d1);
+                    uint32_t rest = stab[i] & (stab[i] - 1);  // the other stabiliser images
+                    while (rest) {
+                        const uint32_t t = __ffs(rest) - 1;
+                        rest &= rest - 1;
+                        local += claim_entry(P.depth,
+                                             (uint64_t)(packed[i] >> 4) * KindTraits<MODE, NEC>::N_EDGE +
+                                                 edge_coord_sym<MODE, NEC>(T, n[i], T.sym_mul[t][packed[i] & 15u]),
+                                             d1);
+                    }
                 }
             }
         }
+        __syncwarp();
     }
     add_count(P.counter, local);
 }
@@ -116,35 +175,11 @@ __global__ void __launch_bounds__(256) bfs_backward(const DevTables* __restrict_
     stage_tables(T, gT);
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     unsigned long long local = 0;
-    const uint4* chunks = reinterpret_cast<const uint4*>(P.depth);
     const uint8_t* depth = P.depth;
     const uint64_t n_groups = (P.n_chunks + 31u) / 32u;
     const uint64_t n_warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
     for (uint64_t gi = blockIdx.x * (uint64_t)(blockDim.x >> 5) + warp; gi < n_groups; gi += n_warps) {
-        const uint64_t ch = gi * 32u + lane;
-        uint32_t unvisited = 0;  // bit j: entry j of this lane's chunk is unvisited
-        if (ch < P.n_chunks) {
-            uint4 v = chunks[ch];
-            uint32_t w[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                uint32_t x = w[q];
-                uint32_t hit = x & (x << 1) & (x << 2) & (x << 3) & (x << 4) & (x << 5) & (x << 6) & (x << 7) &
-                               0x80808080u;  // 0x80 where byte == 0xFF
-                unvisited |= ((((hit >> 7) & 0x01010101u) * 0x01020408u) >> 24) << (4 * q);
-            }
-        }
-        const uint32_t cnt = __popc(unvisited);
-        uint32_t incl = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-            if (lane >= (uint32_t)o) incl += t;
-        }
-        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-        uint32_t pos = incl - cnt;
-        for (uint32_t mm = unvisited; mm; mm &= mm - 1) list[warp][pos++] = (uint16_t)(lane * 16u + (__ffs(mm) - 1));
-        __syncwarp();
+        const uint32_t total = list_group(P, gi, lane, 0xFFu, list[warp]);
         for (uint32_t it = lane; it < total; it += 32u) {
             const uint64_t idx = gi * 512u + list[warp][it];
             if (idx >= P.n_entries) continue;
