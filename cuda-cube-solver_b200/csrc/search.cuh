@@ -9,6 +9,11 @@ constexpr uint32_t SLOT_FREE = 0, SLOT_ACTIVE = 1, SLOT_SOLVED = 2, SLOT_ERROR =
 constexpr unsigned long long TICKET_IDLE = 0x7FFFFFFFull;  // ticket of a slot with no iteration: exhausted
 constexpr int MAX_PLEN = 6;
 constexpr uint32_t RING_RETIRED = 0xFFFFFFFFu;  // ring entry whose iteration is fully handed out
+// A ring entry's low word: slot generation << SLOT_BITS | slot.  A server slot gets a new
+// generation each time it is reused, so an entry left from the slot's previous cube is told apart.
+constexpr uint32_t SLOT_BITS = 20, SLOT_MASK = (1u << SLOT_BITS) - 1u, GEN_MASK = 0xFFFu;
+constexpr uint32_t MAX_SLOTS = SLOT_MASK;       // slot ids below 2^20 - 1 (the all-ones id is RING_RETIRED's)
+constexpr uint32_t QUEUED = 0x80000000u;        // Slot.queued = QUEUED | generation of the live entry
 constexpr uint32_t MAX_BOUND = 22;   // every position is solvable in 20 half-turn moves
 
 // One cube under search.  The ticket is the work counter of the current IDA* iteration
@@ -28,8 +33,9 @@ struct alignas(16) Slot {
     unsigned long long iter_nodes[24];  // nodes per bound
     unsigned long long t_admit, t_done; // device globaltimer, ns
     uint32_t table;                  // 0: the handle's table, 1: its second resident table
-    uint32_t queued;                 // 1 while the work ring holds a live entry for this slot
-    uint32_t pad2[2];
+    uint32_t queued;                 // QUEUED | gen while the work ring holds a live entry for this cube
+    uint32_t gen;                    // generation of the slot (server: incremented on every reuse)
+    uint32_t pad2[1];
 };
 
 struct QueueState {

@@ -87,17 +87,20 @@ __device__ __forceinline__ uint64_t ticket_make(uint32_t plen, uint32_t bound, u
     return ((uint64_t)plen << 56) | ((uint64_t)bound << 48) | ((uint64_t)(epoch & 0xFFFFu) << 32);
 }
 
-__device__ __forceinline__ void enqueue_slot(const SearchParams& P, uint32_t s) {
+// Appends an entry (low word: generation << SLOT_BITS | slot) to the work ring.
+__device__ __forceinline__ void enqueue_entry(const SearchParams& P, uint32_t low) {
     unsigned long long pos = atomicAdd(&P.q->tail, 1ull);
     unsigned long long lap = pos / P.ring_cap;
-    atomicExch(&P.ring[pos % P.ring_cap], (lap << 32) | s);
+    atomicExch(&P.ring[pos % P.ring_cap], (lap << 32) | low);
 }
 
-// A slot has at most one live ring entry: it is queued only when it has none (the flag is cleared
-// by the lane that retires the entry, which then re-checks the ticket, so an iteration published
-// meanwhile is queued by one of the two).
+// A cube has at most one live ring entry: it is queued only when it has none.  The flag holds
+// the generation of the entry; the lane that retires that entry clears it and then re-checks the
+// ticket, so an iteration published meanwhile is queued by one of the two.  An entry left from a
+// reused slot's previous cube carries the old generation and clears nothing.
 __device__ __forceinline__ void queue_slot(const SearchParams& P, uint32_t s) {
-    if (atomicExch(&P.slots[s].queued, 1u) == 0u) enqueue_slot(P, s);
+    const uint32_t gen = *(volatile uint32_t*)&P.slots[s].gen & GEN_MASK;
+    if (atomicCAS(&P.slots[s].queued, 0u, QUEUED | gen) == 0u) enqueue_entry(P, (gen << SLOT_BITS) | s);
 }
 
 __device__ __forceinline__ bool ticket_open(const SearchParams& P, unsigned long long tk) {
@@ -168,7 +171,7 @@ static __device__ __noinline__ void advance_head(const SearchParams& P) {
         if (lap == want && (uint32_t)e != RING_RETIRED) {
             if (t - h < P.ring_cap / 2u) return;  // room left: the live entry stays
             if (atomicCAS(cell, e, (e & 0xFFFFFFFF00000000ull) | RING_RETIRED) != e) return;
-            enqueue_slot(P, (uint32_t)e);
+            enqueue_entry(P, (uint32_t)e);
         }
         atomicCAS((unsigned long long*)&P.q->head, h, h + 1);  // retired, moved or overwritten
     }
@@ -218,8 +221,9 @@ __device__ __forceinline__ int fetch_item(const SearchParams& P, uint32_t seed, 
             unsigned long long* cell = P.ring + pos % P.ring_cap;
             unsigned long long e = *(volatile unsigned long long*)cell;
             if ((e >> 32) == pos / P.ring_cap) {  // written (unwritten or overwritten entries are skipped)
-                uint32_t s = (uint32_t)e;
-                if (s != RING_RETIRED) {
+                const uint32_t low = (uint32_t)e;
+                if (low != RING_RETIRED) {
+                    const uint32_t s = low & SLOT_MASK;
                     unsigned long long tk = atomicAdd(&P.slots[s].ticket, 1ull);
                     uint32_t i = (uint32_t)tk, pl = (uint32_t)(tk >> 56);
                     if (pl <= (uint32_t)MAX_PLEN && i < P.n_prefix[pl]) {
@@ -233,9 +237,11 @@ __device__ __forceinline__ int fetch_item(const SearchParams& P, uint32_t seed, 
                     // iteration handed out: retire the entry; if a new iteration was published
                     // meanwhile (its queue_slot saw this entry still live), queue it now
                     if (atomicCAS(cell, e, (e & 0xFFFFFFFF00000000ull) | RING_RETIRED) == e) {
-                        atomicExch(&P.slots[s].queued, 0u);
-                        __threadfence();
-                        if (ticket_open(P, *(volatile unsigned long long*)&P.slots[s].ticket)) queue_slot(P, s);
+                        const uint32_t flag = QUEUED | (low >> SLOT_BITS);
+                        if (atomicCAS(&P.slots[s].queued, flag, 0u) == flag) {
+                            __threadfence();
+                            if (ticket_open(P, *(volatile unsigned long long*)&P.slots[s].ticket)) queue_slot(P, s);
+                        }
                     }
                 }
                 if (pos == h) atomicCAS((unsigned long long*)&P.q->head, h, h + 1);

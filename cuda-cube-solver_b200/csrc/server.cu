@@ -46,6 +46,7 @@ struct Server {
     unsigned long long admit_pos = 0;
     std::vector<uint32_t> free_slots;
     std::vector<uint64_t> slot_request;
+    std::vector<uint32_t> slot_gen;  // reuse count of each slot
     uint32_t in_flight = 0;
 
     std::mutex mu;
@@ -97,6 +98,7 @@ int Server::step() {
             slot_request[s] = t.first;
             Slot sl;
             make_slot(t.second.data(), (uint32_t)t.first, t.second[5], &sl);
+            sl.gen = ++slot_gen[s] & GEN_MASK;  // tells an entry left from the slot's last cube apart
             CCS_CUDA_TRY(cudaMemcpyAsync(h->d_slots + s, &sl, sizeof sl, cudaMemcpyHostToDevice, copy));
             unsigned long long pos = admit_pos++;
             unsigned long long entry = ((pos / P.admit_cap) << 32) | s;
@@ -164,6 +166,7 @@ int server_stop(ccs_handle* h) {
 
 extern "C" int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* opts) {
     if (!h || slots <= 0) return fail(CCS_E_ARG, "bad arguments");
+    if ((uint32_t)slots >= MAX_SLOTS) return fail(CCS_E_ARG, "%d slots: at most %u", slots, MAX_SLOTS - 1);
     if (!h->d_table) return fail(CCS_E_STATE, "no table loaded");
     if (h->server) return fail(CCS_E_STATE, "server already running");
     CCS_TRY(ensure_search_buffers(h, (uint32_t)slots));
@@ -189,6 +192,7 @@ extern "C" int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* 
     CCS_CUDA_TRY(cudaMemcpyAsync(h->d_q, &q, sizeof q, cudaMemcpyHostToDevice, s->copy));
     CCS_CUDA_TRY(cudaStreamSynchronize(s->copy));
     s->slot_request.assign(h->slot_cap, 0);
+    s->slot_gen.assign(h->slot_cap, 0);
     for (uint32_t i = (uint32_t)slots; i-- > 0;) s->free_slots.push_back(i);
     Server* raw = s.release();
     h->server = raw;

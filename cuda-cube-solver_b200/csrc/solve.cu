@@ -171,6 +171,7 @@ extern "C" int ccs_solve_tables(ccs_handle* h, const uint32_t* states, const uin
     }
     if (h->server) return fail(CCS_E_STATE, "the server owns this handle's search buffers");
     if (n <= 0) return CCS_OK;
+    if ((uint32_t)n >= MAX_SLOTS) return fail(CCS_E_ARG, "%d cubes in one call: at most %u", n, MAX_SLOTS - 1);
     for (int i = 0; i < n; ++i)
         if (!is_legal(unpack(states + 5ull * i))) return fail(CCS_E_ARG, "cube %d is not a legal position", i);
     CCS_TRY(ensure_search_buffers(h, (uint32_t)n));
