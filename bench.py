@@ -219,6 +219,38 @@ def served_stream(args, solver, opts) -> dict:
     return stats
 
 
+def batched_mix(args, solver, opts) -> dict:
+    """Config 4: one batch of ``--batch`` cubes in which 5% are hard positions -- uniform cubes of
+    seed 20 whose optimal length is >= 19 (found by set-up solves) and the superflip -- solved on
+    d4t and, with the second table attached, on d4.  Device time of each batch; the two tables
+    must give the same optimal lengths."""
+
+    from cuda_cube_solver import workloads
+    from cuda_cube_solver.device import state_words
+
+    n = args.batch
+    n_hard = max(2, n * 5 // 100)
+    cubes = workloads.uniform_cubes(n, seed=args.seed + 500)
+    cand = workloads.uniform_cubes(n_hard * 40, seed=20)
+    lengths = [len(sol.moves) for sol in solver.solve(cand)]  # set-up: find the long ones
+    hard = [c for c, L in zip(cand, lengths) if L >= 19][: n_hard - 1] + [workloads.superflip()]
+    where = np.random.default_rng(4).choice(n, size=len(hard), replace=False)
+    for i, c in zip(where, hard):
+        cubes[int(i)] = c
+    words = state_words(cubes)
+    out = {"cubes": n, "hard": len(hard), "length_ge_19": len(hard) - 1, "superflip": 1}
+    runs = [("d4t", 0)] + ([(solver.second_kind, 1)] if solver.second_kind else [])
+    lens = {}
+    for name, tid in runs:
+        res = solver.handle.solve(words, opts, np.full(n, tid, np.uint8))
+        ms, probes, _ = solver.handle.last_solve_stats()
+        lens[name] = [r.length for r in res]
+        out[name] = {"cubes_per_s": n / (ms / 1000.0), "probes_per_s": probes / (ms / 1000.0), "ms": ms}
+    if len(lens) == 2:
+        out["lengths_equal"] = lens["d4t"] == lens[solver.second_kind]
+    return out
+
+
 def build_report(args, solver, peaks) -> dict:
     """The table build of the set-up (GPU BFS + encoding): entries per second and the
     algorithmic DRAM write bandwidth (one depth byte per entry, then the encoded table)."""
@@ -293,6 +325,7 @@ def main() -> None:
     ap.add_argument("--second", default=None,
                     help="second resident table for the served stream (default: d4 beside d4t; 'none' for none)")
     ap.add_argument("--no-ceiling", action="store_true", help="skip the random-sector gather ceiling measurement")
+    ap.add_argument("--mix", type=int, default=1, help="1: also time one batch with 5%% hard positions on d4t and d4")
     args = ap.parse_args()
     if args.second is None:
         args.second = "d4" if args.kind == "d4t" and args.format == "block" else ""
@@ -399,10 +432,11 @@ def main() -> None:
                  "worst_s": max(plain_lat), "probes_per_s": plain_probes / plain_dev if plain_dev else None,
                  "batched_over_plain": value / (len(plain_lat) / sum(plain_lat))}
 
+    if args.second:  # set-up: the second resident table (d4 beside d4t)
+        solver.attach_second(args.second)
+    mix = batched_mix(args, solver, opts) if args.mix else None
     served = None
     if args.serve:
-        if args.second:  # set-up: the second resident table for highly flipped requests
-            solver.attach_second(args.second)
         served = served_stream(args, solver, opts)
 
     peaks = measured_peaks()
@@ -441,7 +475,7 @@ def main() -> None:
                                "move_min": opts.move_min, "move_age": opts.move_age, "probe_min": opts.probe_min,
                                "autotuned": tuned is not None},
            "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
-           "plain": plain, "served": served, "table_build_s": build_s, "table_build_gpu_s": solver.build_seconds,
+           "plain": plain, "batched_mix": mix, "served": served, "table_build_s": build_s, "table_build_gpu_s": solver.build_seconds,
            "table_build": build_report(args, solver, peaks),
            "wall_s_per_step": statistics.mean(wall)}
     print(json.dumps(out))
