@@ -39,27 +39,78 @@ void log_msg(ccs_log_fn log, const char* fmt, ...) {
     log(buf);
 }
 
+// Two pinned staging buffers: the copy of one chunk overlaps the file I/O of the other.
+struct Staging {
+    PinnedBuffer a{CHUNK_BYTES}, b{CHUNK_BYTES};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    bool ok() const { return a.p && b.p && done[0] && done[1]; }
+    Staging() {
+        if (cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming) != cudaSuccess) done[0] = nullptr;
+        if (cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming) != cudaSuccess) done[1] = nullptr;
+    }
+    ~Staging() {
+        if (done[0]) cudaEventDestroy(done[0]);
+        if (done[1]) cudaEventDestroy(done[1]);
+    }
+    void* buf(int i) const { return i ? b.p : a.p; }
+};
+
 int write_device_file(const void* dptr, uint64_t n_bytes, const std::string& path, cudaStream_t stream) {
-    PinnedBuffer buf(CHUNK_BYTES);
-    if (!buf.p) return fail(CCS_E_NOMEM, "pinned staging buffer");
+    Staging st;
+    if (!st.ok()) return fail(CCS_E_NOMEM, "pinned staging buffers");
     std::string tmp = path + ".tmp";  // a crash mid-write must not leave a table that looks complete
     FILE* f = fopen(tmp.c_str(), "wb");
     if (!f) return fail(CCS_E_FILE, "%s: cannot open for writing", tmp.c_str());
-    for (uint64_t off = 0; off < n_bytes; off += CHUNK_BYTES) {
-        size_t n = (size_t)std::min<uint64_t>(CHUNK_BYTES, n_bytes - off);
-        cudaError_t e = cudaMemcpyAsync(buf.p, (const char*)dptr + off, n, cudaMemcpyDeviceToHost, stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-        if (e != cudaSuccess) {
-            fclose(f);
-            return fail(CCS_E_CUDA, "copy to host: %s", cudaGetErrorString(e));
-        }
-        if (fwrite(buf.p, 1, n, f) != n) {
+    const uint64_t n_chunks = (n_bytes + CHUNK_BYTES - 1) / CHUNK_BYTES;
+    auto issue = [&](uint64_t c) -> cudaError_t {  // device -> staging buffer c % 2
+        const uint64_t off = c * CHUNK_BYTES;
+        const size_t n = (size_t)std::min<uint64_t>(CHUNK_BYTES, n_bytes - off);
+        cudaError_t e = cudaMemcpyAsync(st.buf((int)(c & 1)), (const char*)dptr + off, n, cudaMemcpyDeviceToHost, stream);
+        return e == cudaSuccess ? cudaEventRecord(st.done[c & 1], stream) : e;
+    };
+    cudaError_t e = n_chunks ? issue(0) : cudaSuccess;
+    for (uint64_t c = 0; c < n_chunks && e == cudaSuccess; ++c) {
+        if (c + 1 < n_chunks) e = issue(c + 1);
+        if (e == cudaSuccess) e = cudaEventSynchronize(st.done[c & 1]);
+        if (e != cudaSuccess) break;
+        const size_t n = (size_t)std::min<uint64_t>(CHUNK_BYTES, n_bytes - c * CHUNK_BYTES);
+        if (fwrite(st.buf((int)(c & 1)), 1, n, f) != n) {
+            cudaStreamSynchronize(stream);
             fclose(f);
             return fail(CCS_E_FILE, "%s: write failed", tmp.c_str());
         }
     }
+    if (e != cudaSuccess) {
+        cudaStreamSynchronize(stream);
+        fclose(f);
+        return fail(CCS_E_CUDA, "copy to host: %s", cudaGetErrorString(e));
+    }
     if (fclose(f) != 0) return fail(CCS_E_FILE, "%s: close failed", tmp.c_str());
     if (std::rename(tmp.c_str(), path.c_str()) != 0) return fail(CCS_E_FILE, "rename %s -> %s failed", tmp.c_str(), path.c_str());
+    return CCS_OK;
+}
+
+// Reads `n_bytes` of `f` into device memory `d`, the read of one chunk overlapping the copy of
+// the previous one.
+int read_file_to_device(FILE* f, void* d, uint64_t n_bytes, const char* path, cudaStream_t stream) {
+    Staging st;
+    if (!st.ok()) return fail(CCS_E_NOMEM, "pinned staging buffers");
+    for (uint64_t off = 0, c = 0; off < n_bytes; off += CHUNK_BYTES, ++c) {
+        const size_t n = (size_t)std::min<uint64_t>(CHUNK_BYTES, n_bytes - off);
+        void* b = st.buf((int)(c & 1));
+        cudaError_t e = c >= 2 ? cudaEventSynchronize(st.done[c & 1]) : cudaSuccess;  // buffer's last copy done
+        if (e == cudaSuccess && fread(b, 1, n, f) != n) {
+            cudaStreamSynchronize(stream);
+            return fail(CCS_E_FILE, "%s: short read", path);
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync((char*)d + off, b, n, cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess) e = cudaEventRecord(st.done[c & 1], stream);
+        if (e != cudaSuccess) {
+            cudaStreamSynchronize(stream);
+            return fail(CCS_E_CUDA, "copy to device: %s", cudaGetErrorString(e));
+        }
+    }
+    CCS_CUDA_TRY(cudaStreamSynchronize(stream));
     return CCS_OK;
 }
 
@@ -86,26 +137,11 @@ extern "C" int ccs_load_table(ccs_handle* h, const char* kind, int format, const
         fclose(f);
         return fail(CCS_E_NOMEM, "device allocation of %llu bytes for the table", (unsigned long long)want);
     }
-    PinnedBuffer buf(CHUNK_BYTES);
-    if (!buf.p) {
+    const int rc = read_file_to_device(f, d, want, path, h->stream);
+    if (rc != CCS_OK) {
         fclose(f);
         cudaFree(d);
-        return fail(CCS_E_NOMEM, "pinned staging buffer");
-    }
-    for (uint64_t off = 0; off < want; off += CHUNK_BYTES) {
-        size_t n = (size_t)std::min<uint64_t>(CHUNK_BYTES, want - off);
-        if (fread(buf.p, 1, n, f) != n) {
-            fclose(f);
-            cudaFree(d);
-            return fail(CCS_E_FILE, "%s: short read", path);
-        }
-        cudaError_t e = cudaMemcpyAsync((char*)d + off, buf.p, n, cudaMemcpyHostToDevice, h->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-        if (e != cudaSuccess) {
-            fclose(f);
-            cudaFree(d);
-            return fail(CCS_E_CUDA, "copy to device: %s", cudaGetErrorString(e));
-        }
+        return rc;
     }
     fclose(f);
     h->d_table = d;
@@ -154,21 +190,13 @@ extern "C" int ccs_attach_table(ccs_handle* h, const char* kind, int format, con
         fclose(f);
         return fail(CCS_E_NOMEM, "device allocation of %llu bytes for the second table", (unsigned long long)want);
     }
-    PinnedBuffer buf(CHUNK_BYTES);
-    for (uint64_t off = 0; buf.p && off < want; off += CHUNK_BYTES) {
-        size_t n = (size_t)std::min<uint64_t>(CHUNK_BYTES, want - off);
-        if (fread(buf.p, 1, n, f) != n || cudaMemcpy((char*)d + off, buf.p, n, cudaMemcpyHostToDevice) != cudaSuccess) {
-            fclose(f);
-            cudaFree(d);
-            return fail(CCS_E_FILE, "%s: read or copy failed", path_s.c_str());
-        }
-    }
+    int rc = read_file_to_device(f, d, want, path_s.c_str(), h->stream);
     fclose(f);
-    if (!buf.p) {
+    if (rc != CCS_OK) {
         cudaFree(d);
-        return fail(CCS_E_NOMEM, "pinned staging buffer");
+        return rc;
     }
-    int rc = attach_second(h, kind, format, d, want);
+    rc = attach_second(h, kind, format, d, want);
     if (rc != CCS_OK) cudaFree(d);
     return rc;
 }

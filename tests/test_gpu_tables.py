@@ -12,6 +12,8 @@ import pytest
 
 from conftest import GOLDEN, resident_handle
 from cuda_cube_solver import kinds, native
+from cuda_cube_solver.cubie import MOVES_HTM, CubieState, apply_moves
+from cuda_cube_solver.device import state_words
 
 pytestmark = pytest.mark.gpu
 
@@ -88,8 +90,23 @@ def test_file_roundtrip_and_size_check(tmp_path):
     h2 = native.Handle()
     try:
         h2.load_table("304", "block", path)
+        assert _sha(h2.table_copy()) == _sha(table)  # the double-buffered load is byte exact
         words = np.array([[0x03020100, 0x07060504, 0x03020100, 0x07060504, 0x0B0A0908]], np.uint32)
         assert h2.lower_bound(words).tolist() == [0]
+        # the same file attached as a second table answers like the first
+        h2.attach_table("304", "block", path)
+        cubes = state_words([CubieState(), apply_moves(CubieState(), [MOVES_HTM[m] for m in (0, 4, 8, 13, 2, 16)])])
+        first = h2.solve(cubes, native.solve_opts(timeout_s=120))
+        second = h2.solve(cubes, native.solve_opts(timeout_s=120), np.ones(2, np.uint8))
+        assert [r.length for r in first] == [r.length for r in second]
+        # a table written by the build (double-buffered device -> file) equals its device copy
+        out = tmp_path / "built-304.bin"
+        h3 = native.Handle()
+        try:
+            h3.build_table("304", "block", out, keep_resident=True)
+            assert _sha(np.fromfile(out, np.uint8)) == _sha(h3.table_copy()) == _sha(table)
+        finally:
+            h3.close()
         bad = tmp_path / "short.bin"
         table[:1000].tofile(bad)
         with pytest.raises(native.CcsError, match="size 1000"):
