@@ -75,6 +75,7 @@ struct SearchParams {
     uint32_t move_min;               // phased kernel: lanes waiting before a MOVE pass runs
     uint32_t move_age;               // phased kernel: iterations a waiting lane may be deferred
     uint32_t probe_min;              // phased kernel: probe pass repeats while this many lanes probe
+    uint32_t persistent;             // server: an empty queue is not the end (lanes wait for new cubes)
     unsigned long long* done_log;    // host-mapped completion log (server), may be null
     uint32_t done_log_cap;
 };

@@ -154,6 +154,12 @@ __device__ __forceinline__ uint32_t next_plen(const SearchParams& P, unsigned lo
 
 enum FetchResult { FETCH_OK = 0, FETCH_EMPTY = 1, FETCH_FINISHED = 2, FETCH_ADMIT = 3 };
 
+// A server launch has nothing left: no cube admitted and unfinished, none waiting for admission.
+__device__ __forceinline__ bool server_idle(const SearchParams& P) {
+    volatile QueueState* q = P.q;
+    return q->active == 0u && q->admit_head >= q->admit_tail;
+}
+
 // Keeps the ring's head moving so that the queued positions (tail - head) stay well under the
 // capacity: retired entries are passed, and once the ring is half full a live entry at the head
 // (a cube whose long iteration is still being handed out) is moved to the tail instead of holding
@@ -210,7 +216,11 @@ __device__ __forceinline__ int fetch_item(const SearchParams& P, uint32_t seed, 
         }
         advance_head(P);
         unsigned long long h = q->head, t = q->tail;
-        if (h >= t) return (q->active == 0u && q->admit_head >= q->admit_tail) ? FETCH_FINISHED : FETCH_EMPTY;
+        // Batches end when nothing is queued, admitted or in flight; a server's lanes keep
+        // polling instead (a lane that took FETCH_FINISHED would stay idle for the rest of the
+        // launch while new cubes arrive), and its warps leave after the idle limit.
+        if (h >= t)
+            return (!P.persistent && q->active == 0u && q->admit_head >= q->admit_tail) ? FETCH_FINISHED : FETCH_EMPTY;
         // Lanes start at a seeded position among the first `spread` queued iterations and scan
         // forward past handed-out entries, so the lanes spread over many cubes: each cube's items
         // are worked roughly in prefix order and a solution found early stops the rest of its
@@ -509,8 +519,14 @@ f.load(sl.frame);
             // No lane has a probe: the warp backs off; after too many empty polls in a row it
             // leaves (warp-uniform counter), and the host relaunches while cubes remain.
             if (++idle_polls > P.idle_limit) {
-                if (lane == 0) atomicOr(&P.q->error, ERR_IDLE_LIMIT);
-                break;
+                // A batch launch leaves (the host relaunches while cubes remain); a server launch
+                // leaves only when no cube is in flight, so every warp stays to serve new work.
+                if (!P.persistent) {
+                    if (lane == 0) atomicOr(&P.q->error, ERR_IDLE_LIMIT);
+                    break;
+                }
+                if (__shfl_sync(0xFFFFFFFFu, (int)server_idle(P), 0)) break;
+                idle_polls = 0;
             }
             if ((idle_polls & 1023u) == 64u && lane == 0) requeue_stranded(P);
             __nanosleep(backoff);

@@ -213,8 +213,14 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
         if (__ballot_sync(0xFFFFFFFFu, eval || have) == 0u) {
             // Nothing queued for this warp: back off; leave after too many empty polls in a row.
             if (++idle_polls > P.idle_limit) {
-                if (lane == 0) atomicOr(&P.q->error, ERR_IDLE_LIMIT);
-                break;
+                // A batch launch leaves (the host relaunches while cubes remain); a server launch
+                // leaves only when no cube is in flight, so every warp stays to serve new work.
+                if (!P.persistent) {
+                    if (lane == 0) atomicOr(&P.q->error, ERR_IDLE_LIMIT);
+                    break;
+                }
+                if (__shfl_sync(0xFFFFFFFFu, (int)server_idle(P), 0)) break;
+                idle_polls = 0;
             }
             if ((idle_polls & 1023u) == 64u && lane == 0) requeue_stranded(P);
             __nanosleep(backoff);

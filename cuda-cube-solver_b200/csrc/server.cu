@@ -182,6 +182,8 @@ extern "C" int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* 
     CCS_CUDA_TRY(cudaHostGetDevicePointer(&s->d_done_log, s->done_log, 0));
     fill_params(h, opts, &s->P);
     s->P.n_slots = (uint32_t)slots;
+    s->P.persistent = 1;
+    s->P.idle_limit = 1u << 16;  // ~0.25 s of idle polling, then the launch ends (relaunched on demand)
     s->P.done_log = s->d_done_log;
     s->P.done_log_cap = s->log_cap;
     s->variant = resolve_variant(opts, 0);
