@@ -138,16 +138,20 @@ __device__ __forceinline__ void finish_slot(const SearchParams& P, uint32_t s, u
 // Prefix length of the next iteration: base, plus one per "deeper" threshold the last iteration
 // reached (a few huge subtrees would otherwise leave the GPU idle), minus one per "shallow"
 // threshold it stayed under when many cubes are active (tiny items cost more to fetch than to
-// search, and other cubes fill the lanes), at most the bound.
+// search, and other cubes fill the lanes), at most the bound.  While few cubes are in flight the
+// deeper thresholds are divided by P.few_divisor: a lone hard cube then gets the GPU's lanes in
+// smaller items and its iterations end on shorter stragglers.
 __device__ __forceinline__ uint32_t next_plen(const SearchParams& P, unsigned long long last_nodes, uint32_t bound) {
-    uint32_t pl = P.base_plen + (last_nodes >= P.deeper_at[0]) + (last_nodes >= P.deeper_at[1]);
     // cubes admitted and not finished (q->active also counts admissions being attempted, which
     // briefly overshoots when many lanes race for the admission ring)
     volatile QueueState* q = P.q;
     const unsigned long long fin = q->finished;  // read first: then fin <= admitted
     const unsigned long long in_flight = q->admit_head - fin;
-    if (in_flight >= P.shallow_min_active)  // enough cubes to keep lanes busy
-        pl -= (uint32_t)(last_nodes < P.shallow_at[0]) + (uint32_t)(last_nodes < P.shallow_at[1]);
+    const bool many = in_flight >= P.shallow_min_active;  // enough cubes to keep lanes busy
+    const unsigned long long d0 = many ? P.deeper_at[0] : P.deeper_at[0] / P.few_divisor;
+    const unsigned long long d1 = many ? P.deeper_at[1] : P.deeper_at[1] / P.few_divisor;
+    uint32_t pl = P.base_plen + (last_nodes >= d0) + (last_nodes >= d1);
+    if (many) pl -= (uint32_t)(last_nodes < P.shallow_at[0]) + (uint32_t)(last_nodes < P.shallow_at[1]);
     pl = pl < 1u ? 1u : (pl > (uint32_t)MAX_PLEN ? (uint32_t)MAX_PLEN : pl);
     return pl < bound ? pl : bound;
 }
