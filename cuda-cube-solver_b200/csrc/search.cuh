@@ -70,7 +70,8 @@ struct SearchParams {
     unsigned long long deeper_at[2]; // an iteration of at least this many nodes -> one move longer
     unsigned long long shallow_at[2]; // an iteration of fewer nodes -> one move shorter (0: off)
     uint32_t shallow_min_active;     // ... applied only while at least this many cubes are active
-    uint32_t few_divisor;            // below that many, the deeper thresholds are divided by this
+    uint32_t few_max_active;         // with at most this many cubes in flight ...
+    uint32_t few_divisor;            // ... the deeper thresholds are divided by this
     uint32_t idle_limit;             // idle polls before a warp leaves (kernel relaunched by the host)
     uint32_t spread;                 // lanes take items from up to this many queued iterations
     uint32_t move_min;               // phased kernel: lanes waiting before a MOVE pass runs

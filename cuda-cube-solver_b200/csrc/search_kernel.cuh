@@ -138,9 +138,10 @@ __device__ __forceinline__ void finish_slot(const SearchParams& P, uint32_t s, u
 // Prefix length of the next iteration: base, plus one per "deeper" threshold the last iteration
 // reached (a few huge subtrees would otherwise leave the GPU idle), minus one per "shallow"
 // threshold it stayed under when many cubes are active (tiny items cost more to fetch than to
-// search, and other cubes fill the lanes), at most the bound.  While few cubes are in flight the
-// deeper thresholds are divided by P.few_divisor: a lone hard cube then gets the GPU's lanes in
-// smaller items and its iterations end on shorter stragglers.
+// search, and other cubes fill the lanes), at most the bound.  While at most P.few_max_active
+// cubes are in flight the deeper thresholds are divided by P.few_divisor: a lone hard cube then
+// gets the GPU's lanes in smaller items and its iterations end on shorter stragglers (with more
+// cubes sharing the GPU, the extra items cost more than they balance).
 __device__ __forceinline__ uint32_t next_plen(const SearchParams& P, unsigned long long last_nodes, uint32_t bound) {
     // cubes admitted and not finished (q->active also counts admissions being attempted, which
     // briefly overshoots when many lanes race for the admission ring)
@@ -148,8 +149,9 @@ __device__ __forceinline__ uint32_t next_plen(const SearchParams& P, unsigned lo
     const unsigned long long fin = q->finished;  // read first: then fin <= admitted
     const unsigned long long in_flight = q->admit_head - fin;
     const bool many = in_flight >= P.shallow_min_active;  // enough cubes to keep lanes busy
-    const unsigned long long d0 = many ? P.deeper_at[0] : P.deeper_at[0] / P.few_divisor;
-    const unsigned long long d1 = many ? P.deeper_at[1] : P.deeper_at[1] / P.few_divisor;
+    const bool few = in_flight <= P.few_max_active;       // one or two cubes own the GPU
+    const unsigned long long d0 = few ? P.deeper_at[0] / P.few_divisor : P.deeper_at[0];
+    const unsigned long long d1 = few ? P.deeper_at[1] / P.few_divisor : P.deeper_at[1];
     uint32_t pl = P.base_plen + (last_nodes >= d0) + (last_nodes >= d1);
     if (many) pl -= (uint32_t)(last_nodes < P.shallow_at[0]) + (uint32_t)(last_nodes < P.shallow_at[1]);
     pl = pl < 1u ? 1u : (pl > (uint32_t)MAX_PLEN ? (uint32_t)MAX_PLEN : pl);
