@@ -183,6 +183,9 @@ extern "C" int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* 
     fill_params(h, opts, &s->P);
     s->P.n_slots = (uint32_t)slots;
     s->P.persistent = 1;
+    // Served cubes keep the plain deeper thresholds: with the few-cube rule on, the served
+    // stream's p50 rose from 43 to 131 ms on B200 (it pays off for a lone batch or plain solve).
+    s->P.few_max_active = 0;
     s->P.idle_limit = 1u << 16;  // ~0.25 s of idle polling, then the launch ends (relaunched on demand)
     s->P.done_log = s->d_done_log;
     s->P.done_log_cap = s->log_cap;
