@@ -1,0 +1,88 @@
+"""Host logic without a GPU: the autotuner's coordinate descent and its cache, and the served
+stream's replay loop and latency statistics, driven by fakes of the library handle and server."""
+
+from __future__ import annotations
+
+import json
+
+import numpy as np
+
+from cuda_cube_solver import autotune, serving, workloads
+
+
+class FakeHandle:
+    """Device time of a solve as a function of the settings, smallest at BEST."""
+
+    BEST = {"variant": 2, "base_plen": 4, "move": (4, 2), "spread": 1024, "probe_min": 12}
+
+    def __init__(self):
+        self.calls = []
+        self._ms = 0.0
+
+    def solve(self, words, opts):
+        self.calls.append(opts)
+        cfg = {"variant": opts.variant, "base_plen": opts.base_plen, "move": (opts.move_min, opts.move_age),
+               "spread": opts.spread, "probe_min": opts.probe_min}
+        self._ms = 100.0 + sum(0.0 if cfg[k] == v else 7.0 + abs(hash((k, cfg[k]))) % 5 for k, v in self.BEST.items())
+        return []
+
+    def last_solve_stats(self):
+        return self._ms, 0, 1
+
+
+def test_autotune_finds_the_best_settings():
+    h = FakeHandle()
+    sample = workloads.uniform_cubes(8, seed=9)
+    result = autotune.tune(h, sample, "d4t", rounds=2)
+    assert result["config"] == FakeHandle.BEST
+    assert result["cubes_per_s"] == len(sample) / 0.1
+    assert result["trials"] == len(h.calls) - 1  # the first call is the warm-up
+    assert result["cubes_per_s"] >= result["default_cubes_per_s"]
+
+
+def test_autotune_cache_round_trip(tmp_path, monkeypatch):
+    monkeypatch.setattr(autotune, "CACHE", tmp_path / "tune" / "cache.json")
+    result = {"config": dict(FakeHandle.BEST, move=list(FakeHandle.BEST["move"])), "cubes_per_s": 1.0}
+    autotune.save(result, "d4t", 1000)
+    assert autotune.lookup("d4t", 500) == FakeHandle.BEST  # same batch-size bucket (64..1023)
+    assert autotune.lookup("d4t", 10) is None  # another bucket
+    assert autotune.lookup("d4", 1000) is None  # another table
+    data = json.loads((tmp_path / "tune" / "cache.json").read_text())
+    assert len(data) == 1 and next(iter(data)).endswith("|d4t|medium")
+    assert [autotune.batch_bucket(n) for n in (1, 10, 100, 5000)] == ["1", "small", "medium", "large"]
+
+
+class FakeServer:
+    """Finishes request i after a fixed device latency of (i % 3 + 1) ms of host time."""
+
+    def __init__(self):
+        self.t = 0.0
+        self.submitted = {}
+        self.next_id = 7
+
+    def submit(self, state):
+        rid = self.next_id
+        self.next_id += 1
+        self.submitted[rid] = serving.time.perf_counter()
+        return rid
+
+    def poll(self):
+        now = serving.time.perf_counter()
+        out = []
+        for rid, t0 in list(self.submitted.items()):
+            if now - t0 >= ((rid - 7) % 3 + 1) * 1e-3:
+                del self.submitted[rid]
+                out.append(serving.Served(rid, 18, [0] * 18, now - t0, 0.0, 1))
+        return out
+
+
+def test_replay_reports_every_request_in_submission_order():
+    cubes = workloads.uniform_cubes(30, seed=3)
+    arrivals = serving.poisson_arrivals(len(cubes), 2000.0, seed=3)
+    stats = serving.replay(FakeServer(), cubes, arrivals, timeout_s=30.0)
+    assert stats["requests"] == 30
+    assert [r.request for r in stats["results"]] == list(range(7, 37))
+    lat = np.array([r.latency_s for r in stats["results"]])
+    assert stats["p50_s"] == float(np.percentile(lat, 50)) and stats["max_s"] == float(lat.max())
+    assert 0.0 < stats["p50_s"] <= stats["p95_s"] <= stats["p99_s"] <= stats["max_s"]
+    assert lat.min() >= 1e-3
