@@ -164,7 +164,31 @@ def cpu_arm(args, states, frames_words, table: np.ndarray, probes_per_cube: floa
             "sample": f"first {n} cubes of the workload, CPU oracle IDA* (oracle/ccs_oracle.c) on {threads} threads for "
                       f"{dt:.1f} s: {int(done.sum())} solved, unfinished work counted at "
                       f"{per_cube / 1e6 if per_cube else 0:.1f} M probes per cube",
-            "probes_per_s": float(probes.sum()) / dt}
+            "probes_per_s": float(probes.sum()) / dt, "probes_per_cube": per_cube}
+
+
+def reference_cpu_gather(probes_per_cube: float | None) -> dict | None:
+    """The reference's own CPU probe benchmark (its bench/cpu_gather.c, compiled from its checkout
+    into oracle/_ref/): random byte lookups in a 7.3 GiB buffer on all host threads and on one,
+    each bounded to a few seconds; with the search's probes per cube it bounds what a CPU search
+    could reach."""
+
+    exe = ROOT / "oracle" / "_ref" / "cpu_gather"
+    if not exe.exists():
+        return None
+    out = {"source": "reference bench/cpu_gather.c", "gib": 7.3}
+    for threads, iters in ((os.cpu_count() or 1, 400000), (1, 1000000)):
+        try:
+            line = subprocess.run([str(exe), "7.3", str(threads), str(iters)], capture_output=True, text=True,
+                                  timeout=120).stdout.strip()
+            rate = float(line.split()[-3]) * 1e9
+        except (subprocess.SubprocessError, ValueError, IndexError):
+            return None
+        out[f"lookups_per_s_{'all' if threads > 1 else 1}"] = rate
+        out["threads"] = out.get("threads", threads)
+    if probes_per_cube:
+        out["cubes_per_s_bound"] = out["lookups_per_s_all"] / probes_per_cube
+    return out
 
 
 def served_stream(args, solver, opts) -> dict:
@@ -365,7 +389,8 @@ def main() -> None:
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/u32 integer",
                "data": "synthetic", "config": config, "impl": "reference",
                "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
-               "e2e": {"value": cpu["value"], "unit": "cubes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+               "e2e": {"value": cpu["value"], "unit": "cubes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+               "reference_cpu_gather": reference_cpu_gather(cpu.get("probes_per_cube"))}
         print(json.dumps(out))
         return
 
