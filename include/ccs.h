@@ -139,7 +139,7 @@ typedef struct ccs_result {
 } ccs_result;
 
 /* Solve n cubes together (GpuSolver.solve, solver.py:254-320): one persistent launch advances
- * every cube through its IDA* bounds on the device.  results[n]. */
+ * every cube through its IDA* bounds on the device.  results[n]; n < 1,048,575 per call. */
 int ccs_solve(ccs_handle* h, const uint32_t* states, int n, const ccs_solve_opts* opts, ccs_result* results);
 
 /* ccs_solve with a table per cube: table_ids[n] of 0 (the first table) or 1 (the attached one). */
@@ -174,7 +174,8 @@ int ccs_probe_bench(ccs_handle* h, int n_states, int rounds, double* probes_per_
  * ccs_server_start runs a service thread that owns a persistent search launch over `slots`
  * cube slots; ccs_server_submit queues a cube (returns a request id), ccs_server_poll returns
  * up to max_out finished results with their request ids.  Cubes that arrive while others are on
- * the GPU are admitted into free slots without waiting for the running ones. */
+ * the GPU are admitted into free slots without waiting for the running ones.  slots <
+ * 1,048,575; each takes 456 bytes of device memory (cube slot and ring positions). */
 int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* opts);
 int ccs_server_submit(ccs_handle* h, const uint32_t* state, uint64_t* request_id);
 int ccs_server_submit_table(ccs_handle* h, const uint32_t* state, int table_id, uint64_t* request_id);
