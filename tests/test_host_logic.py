@@ -86,3 +86,37 @@ def test_replay_reports_every_request_in_submission_order():
     assert stats["p50_s"] == float(np.percentile(lat, 50)) and stats["max_s"] == float(lat.max())
     assert 0.0 < stats["p50_s"] <= stats["p95_s"] <= stats["p99_s"] <= stats["max_s"]
     assert lat.min() >= 1e-3
+
+
+class FakeServerHandle:
+    """Records what serving.Server submits to the library."""
+
+    def __init__(self):
+        self.started = None
+        self.submits = []
+
+    def server_start(self, slots, opts):
+        self.started = slots
+
+    def server_submit(self, words, table_id=0):
+        self.submits.append((np.asarray(words).copy(), table_id))
+        return len(self.submits)
+
+    def server_stop(self):
+        self.started = None
+
+
+def test_server_picks_the_second_table_by_the_flip_rule():
+    h = FakeServerHandle()
+    srv = serving.Server(h, 16, None, flip_rule=12)
+    srv.submit(workloads.superflip())
+    for c in workloads.uniform_cubes(20, seed=11):
+        srv.submit(c)
+    srv.close()
+    assert h.submits[0][1] == 1  # all twelve edges flipped: the d4 table
+    assert all(t == 0 for _, t in h.submits[1:])  # uniform cubes with fewer flips stay on d4t
+    plain = FakeServerHandle()
+    srv = serving.Server(plain, 16, None)  # no second table: always table 0
+    srv.submit(workloads.superflip())
+    srv.close()
+    assert plain.submits[0][1] == 0 and h.started is None
