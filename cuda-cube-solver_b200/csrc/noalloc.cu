@@ -13,8 +13,11 @@
 //
 // Limits: at most CCS_NOALLOC_MAX_CUBES cubes per call; prefixes of at most NOALLOC_MAX_PLEN
 // moves, so an iteration of a very large tree keeps the base prefix length instead of a longer
-// one (deeper_at0/1 are ignored); the first table only.  One array per process and device: calls
-// that overlap on the GPU (two threads, or two handles on one device) race on it.
+// one (deeper_at0/1 are ignored); the first table only; at most NA_MAX_DEVICES devices.  One
+// array per process and device, shared by every handle on that device: calls on one device are
+// serialised by a per-device lock (they would race on the array otherwise), and the host staging
+// is per device too, so calls on different devices run side by side.  A device reset reloads the
+// array zeroed; a marker word in it tells the next call to set it up again.
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -43,10 +46,13 @@ constexpr uint32_t NA_RING = 4 * NA_SLOTS + 64;  // the allocating path's sizing
 constexpr uint32_t NA_PREFIX_COUNT[NOALLOC_MAX_PLEN + 1] = {1, 18, 243, 3240, 43254};
 constexpr uint32_t NA_PREFIX_TOTAL = 1 + 18 + 243 + 3240 + 43254;
 
+constexpr uint32_t NA_MARKER = 0x43435331u;  // "CCS1": the array has been set up on this device
+
 struct NoAllocScratch {
     Slot slots[NA_SLOTS];
     QueueState q;
-    uint32_t pad[4];
+    uint32_t marker;  // NA_MARKER once the prefix lists are in place
+    uint32_t pad[3];
     unsigned long long ring[NA_RING + NA_SLOTS];  // work ring, then the admission ring
     uint32_t prefix[NA_PREFIX_TOTAL];
 };
@@ -56,14 +62,19 @@ static_assert(sizeof(NoAllocScratch) <= 320u * 1024u, "the fixed search buffers 
 // 304 KB of device memory, held by every GPU that loads the library until the process exits.
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
-constexpr int NA_MAX_DEVICES = 64;
-NoAllocScratch* g_scratch_ptr[NA_MAX_DEVICES] = {};  // device addresses, set up once per device
-std::mutex g_setup_mutex;
+constexpr int NA_MAX_DEVICES = 16;
 
-// host staging (file scope: nothing is allocated per call)
-Slot g_host_slots[NA_SLOTS];
-unsigned long long g_host_admit[NA_SLOTS];
-uint32_t g_host_prefix[NA_PREFIX_TOTAL];
+// Per device: the array's device address (found at set-up), the lock that serialises calls, and
+// the host staging of a call (file scope: nothing is allocated per call).
+struct DeviceState {
+    NoAllocScratch* scratch = nullptr;
+    std::mutex mu;
+    Slot slots[NA_SLOTS];
+    unsigned long long admit[NA_SLOTS];
+};
+DeviceState g_dev[NA_MAX_DEVICES];
+uint32_t g_host_prefix[NA_PREFIX_TOTAL];  // written once, under g_prefix_mutex
+std::mutex g_prefix_mutex;
 
 // Canonical sequences of length `len` in lexicographic move order (the order of
 // canonical_prefixes), 5 bits per move, first move lowest; returns the next free position.
@@ -80,24 +91,37 @@ uint32_t enumerate_prefixes(int len, int depth, int last, uint32_t seq, uint32_t
     return pos;
 }
 
-// With `device` current: the array's device address, found and filled with the prefix lists on
-// the first call for this device.
-int setup_device(int device, NoAllocScratch** out) {
-    if (device < 0 || device >= NA_MAX_DEVICES) return fail(CCS_E_ARG, "device %d out of range", device);
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[device]) {
+// With `device` current and its lock held: the array's device address, found and filled with the
+// prefix lists on the first call for this device, and again after a device reset (the reloaded
+// array has no marker).  The copies run on `st` and are complete when this returns.
+int setup_device(int device, cudaStream_t st, NoAllocScratch** out) {
+    DeviceState& D = g_dev[device];
+    if (D.scratch) {
+        uint32_t marker = 0;
+        CCS_CUDA_TRY(cudaMemcpyAsync(&marker, &D.scratch->marker, sizeof marker, cudaMemcpyDeviceToHost, st));
+        CCS_CUDA_TRY(cudaStreamSynchronize(st));
+        if (marker != NA_MARKER) D.scratch = nullptr;
+    }
+    if (!D.scratch) {
         NoAllocScratch* p = nullptr;
         CCS_CUDA_TRY(cudaGetSymbolAddress((void**)&p, g_noalloc_scratch));
-        uint32_t pos = 0;
-        for (int L = 0; L <= NOALLOC_MAX_PLEN; ++L) {
-            uint32_t end = enumerate_prefixes(L, 0, -1, 0u, g_host_prefix, pos);
-            if (end - pos != NA_PREFIX_COUNT[L]) return fail(CCS_E_CHECK, "prefix count of length %d", L);
-            pos = end;
+        {
+            std::lock_guard<std::mutex> lock(g_prefix_mutex);
+            uint32_t pos = 0;
+            for (int L = 0; L <= NOALLOC_MAX_PLEN; ++L) {
+                uint32_t end = enumerate_prefixes(L, 0, -1, 0u, g_host_prefix, pos);
+                if (end - pos != NA_PREFIX_COUNT[L]) return fail(CCS_E_CHECK, "prefix count of length %d", L);
+                pos = end;
+            }
+            CCS_CUDA_TRY(cudaMemcpyAsync(p->prefix, g_host_prefix, sizeof g_host_prefix, cudaMemcpyHostToDevice, st));
+            CCS_CUDA_TRY(cudaStreamSynchronize(st));
         }
-        CCS_CUDA_TRY(cudaMemcpy(p->prefix, g_host_prefix, sizeof g_host_prefix, cudaMemcpyHostToDevice));
-        g_scratch_ptr[device] = p;
+        static const uint32_t marker = NA_MARKER;
+        CCS_CUDA_TRY(cudaMemcpyAsync(&p->marker, &marker, sizeof marker, cudaMemcpyHostToDevice, st));
+        CCS_CUDA_TRY(cudaStreamSynchronize(st));
+        D.scratch = p;
     }
-    *out = g_scratch_ptr[device];
+    *out = D.scratch;
     return CCS_OK;
 }
 
@@ -113,16 +137,21 @@ extern "C" int ccs_solve_noalloc(ccs_handle* h, const uint32_t* states, int n, c
     if (opts && opts->base_plen > NOALLOC_MAX_PLEN)
         return fail(CCS_E_ARG, "base_plen %d: ccs_solve_noalloc takes prefixes of at most %d moves",
                     opts->base_plen, NOALLOC_MAX_PLEN);
-    CCS_CUDA_TRY(cudaSetDevice(h->device));
-    NoAllocScratch* S = nullptr;
-    CCS_TRY(setup_device(h->device, &S));
-    if (n == 0) return CCS_OK;
+    if (h->device < 0 || h->device >= NA_MAX_DEVICES)
+        return fail(CCS_E_ARG, "device %d: ccs_solve_noalloc serves devices 0..%d", h->device, NA_MAX_DEVICES - 1);
     for (int i = 0; i < n; ++i)
         if (!is_legal(unpack(states + 5ull * i))) return fail(CCS_E_ARG, "cube %d is not a legal position", i);
+    CCS_CUDA_TRY(cudaSetDevice(h->device));
+    DeviceState& D = g_dev[h->device];
+    std::lock_guard<std::mutex> lock(D.mu);  // one call at a time per device: they share the array
+    cudaStream_t st = h->stream;
+    NoAllocScratch* S = nullptr;
+    CCS_TRY(setup_device(h->device, st, &S));
+    if (n == 0) return CCS_OK;
 
     for (int i = 0; i < n; ++i) {
-        make_slot(states + 5ull * i, (uint32_t)i, 0u, &g_host_slots[i]);
-        g_host_admit[i] = (unsigned long long)i;  // lap 0
+        make_slot(states + 5ull * i, (uint32_t)i, 0u, &D.slots[i]);
+        D.admit[i] = (unsigned long long)i;  // lap 0
     }
     QueueState q;
     std::memset(&q, 0, sizeof q);
@@ -146,13 +175,13 @@ extern "C" int ccs_solve_noalloc(ccs_handle* h, const uint32_t* states, int n, c
     }
     // every iteration stays at or below the base prefix length: no longer lists exist here
     P.deeper_at[0] = P.deeper_at[1] = ~0ull;
+    P.max_plen = NOALLOC_MAX_PLEN;
 
     // The array keeps the previous call's contents: the slots of this call, the queue state and
     // both rings are rewritten before the launch.
-    cudaStream_t st = h->stream;
-    CCS_CUDA_TRY(cudaMemcpyAsync(S->slots, g_host_slots, sizeof(Slot) * n, cudaMemcpyHostToDevice, st));
+    CCS_CUDA_TRY(cudaMemcpyAsync(S->slots, D.slots, sizeof(Slot) * n, cudaMemcpyHostToDevice, st));
     CCS_CUDA_TRY(cudaMemsetAsync(S->ring, 0xFF, sizeof S->ring, st));
-    CCS_CUDA_TRY(cudaMemcpyAsync(P.admit, g_host_admit, 8ull * n, cudaMemcpyHostToDevice, st));
+    CCS_CUDA_TRY(cudaMemcpyAsync(P.admit, D.admit, 8ull * n, cudaMemcpyHostToDevice, st));
     CCS_CUDA_TRY(cudaMemcpyAsync(&S->q, &q, sizeof q, cudaMemcpyHostToDevice, st));
 
     const int variant = resolve_variant(opts, n);
@@ -184,9 +213,9 @@ extern "C" int ccs_solve_noalloc(ccs_handle* h, const uint32_t* states, int n, c
     h->last_kernel_ms = kernel_ms;
     h->last_probes = q.probes;
     h->last_launches = launches;
-    CCS_CUDA_TRY(cudaMemcpyAsync(g_host_slots, S->slots, sizeof(Slot) * n, cudaMemcpyDeviceToHost, st));
+    CCS_CUDA_TRY(cudaMemcpyAsync(D.slots, S->slots, sizeof(Slot) * n, cudaMemcpyDeviceToHost, st));
     CCS_CUDA_TRY(cudaStreamSynchronize(st));
-    for (int i = 0; i < n; ++i) fill_result(g_host_slots[i], &results[i]);
+    for (int i = 0; i < n; ++i) fill_result(D.slots[i], &results[i]);
     if (q.error & ERR_BOUND) return fail(CCS_E_CHECK, "a search passed the largest possible bound");
     return CCS_OK;
 }

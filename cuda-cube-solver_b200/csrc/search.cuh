@@ -67,6 +67,7 @@ struct SearchParams {
     const uint32_t* prefixes[MAX_PLEN + 1];  // canonical move sequences, 5 bits per move
     uint32_t n_prefix[MAX_PLEN + 1];
     uint32_t base_plen;              // prefix length of a cube's first iterations
+    uint32_t max_plen;               // longest prefix length whose list is present (<= MAX_PLEN)
     unsigned long long deeper_at[2]; // an iteration of at least this many nodes -> one move longer
     unsigned long long shallow_at[2]; // an iteration of fewer nodes -> one move shorter (0: off)
     uint32_t shallow_min_active;     // ... applied only while at least this many cubes are active

@@ -152,10 +152,12 @@ __device__ __forceinline__ uint32_t next_plen(const SearchParams& P, unsigned lo
     const bool few = in_flight <= P.few_max_active;       // one or two cubes own the GPU
     const unsigned long long d0 = few ? P.deeper_at[0] / P.few_divisor : P.deeper_at[0];
     const unsigned long long d1 = few ? P.deeper_at[1] / P.few_divisor : P.deeper_at[1];
-    uint32_t pl = P.base_plen + (last_nodes >= d0) + (last_nodes >= d1);
-    if (many) pl -= (uint32_t)(last_nodes < P.shallow_at[0]) + (uint32_t)(last_nodes < P.shallow_at[1]);
-    pl = pl < 1u ? 1u : (pl > (uint32_t)MAX_PLEN ? (uint32_t)MAX_PLEN : pl);
-    return pl < bound ? pl : bound;
+    // signed: a base of 1 minus two shallow steps is -1, clamped to 1 (never a wrapped length)
+    int pl = (int)P.base_plen + (int)(last_nodes >= d0) + (int)(last_nodes >= d1);
+    if (many) pl -= (int)(last_nodes < P.shallow_at[0]) + (int)(last_nodes < P.shallow_at[1]);
+    const int top = (int)P.max_plen;  // the longest prefix length with a list in this launch
+    pl = pl < 1 ? 1 : (pl > top ? top : pl);
+    return (uint32_t)pl < bound ? (uint32_t)pl : bound;
 }
 
 enum FetchResult { FETCH_OK = 0, FETCH_EMPTY = 1, FETCH_FINISHED = 2, FETCH_ADMIT = 3 };

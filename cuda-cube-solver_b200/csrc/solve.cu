@@ -62,6 +62,7 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
     }
     int base = o && o->base_plen > 0 ? o->base_plen : 4;
     P->base_plen = (uint32_t)std::min(base, MAX_PLEN);
+    P->max_plen = (uint32_t)MAX_PLEN;
     P->deeper_at[0] = (unsigned long long)(o && o->deeper_at0 > 0 ? o->deeper_at0 : 5e7);
     P->deeper_at[1] = (unsigned long long)(o && o->deeper_at1 > 0 ? o->deeper_at1 : 3e9);
     // Small iterations get shorter prefixes (fewer, larger items: fewer fetches); negative = off.

@@ -6,9 +6,11 @@ non-E edges and the E-edge content (labels in position order with their flips, a
 the signed permutation group B4) up to a relabelling group L <= B4.  L must be normalised by the
 relabelling the 16 U-D symmetries induce, or symmetry reduction would be wrong.
 
-Restates ``src/cuda_cube_solver/kinds.py:1-225`` of the reference.  The numbering of the E-content
-classes (``GroupKind.gen``) and the preset list fix the table layout and the drop-in names, so
-both are kept identical; the group closure and class search are written here independently.
+Same interface as ``src/cuda_cube_solver/kinds.py:1-225`` of the reference.  The numbering of
+the E-content classes (``GroupKind.gen``) and the preset list fix the table layout and the drop-in
+names, so both are kept identical; the classes are found here as orbits of the generators'
+relabelling maps on the 384 contents (no group enumeration), and the preset chooser scans the
+ladder from the fastest preset down.
 """
 
 from __future__ import annotations
@@ -21,52 +23,66 @@ import numpy as np
 
 from cuda_cube_solver import coords
 
-PERMS = coords.PERMS4
-PRANK = {p: i for i, p in enumerate(PERMS)}
-IDENT = ((0, 1, 2, 3), (0, 0, 0, 0))
-
-Element = tuple[tuple[int, ...], tuple[int, ...]]
+N_CONTENT = 24 * 16  # E contents: 24 label orders x 16 flip patterns
 
 
-def _mul(a: Element, b: Element) -> Element:
-    """``a`` after ``b``; an element (perm, flips) sends label x to perm[x] and toggles its flip by flips[x]."""
+def _content_index(order: np.ndarray, flips: np.ndarray) -> np.ndarray:
+    """Content number ``rank(order) * 16 + flips`` of label orders (..., 4) and flip bits (..., 4)."""
 
-    (pa, fa), (pb, fb) = a, b
-    return tuple(pa[pb[x]] for x in range(4)), tuple(fb[x] ^ fa[pb[x]] for x in range(4))
-
-
-def _inverse(a: Element) -> Element:
-    p, f = a
-    q = tuple(p.index(z) for z in range(4))
-    return q, tuple(f[q[z]] for z in range(4))
+    code = (order.astype(np.int64) << (2 * np.arange(4))).sum(axis=-1)
+    return coords.EORDER_RANK[code].astype(np.int64) * 16 + (flips.astype(np.int64) << np.arange(4)).sum(axis=-1)
 
 
-def _sym_image() -> set[Element]:
-    """The relabellings of the E edges (cubies 8..11) that the 16 U-D symmetries induce."""
-
-    return {(tuple(int(es.perm[8 + x]) - 8 for x in range(4)), tuple(int(es.flip[8 + x]) for x in range(4)))
-            for es in coords.ud_actions()[1]}
+# Every content as (labels in position order, flips by position): row c of each table.
+_ORDERS = np.array([coords.PERMS4[c >> 4] for c in range(N_CONTENT)], dtype=np.int64)
+_FLIPS = np.array([[(c >> i) & 1 for i in range(4)] for c in range(N_CONTENT)], dtype=np.int64)
 
 
-def _closure(gens) -> set[Element]:
-    group = {IDENT}
-    frontier = [IDENT]
-    while frontier:
-        new = {_mul(g, x) for x in frontier for g in gens} - group
-        group |= new
-        frontier = list(new)
-    return group
+def relabel_action(perm, flips) -> np.ndarray:
+    """The relabelling ``label x -> perm[x]``, flipping the label's edge when ``flips[x]``, as a
+    map of the 384 contents (int array: content -> relabelled content)."""
+
+    perm, flips = np.asarray(perm, np.int64), np.asarray(flips, np.int64)
+    return _content_index(perm[_ORDERS], _FLIPS ^ flips[_ORDERS])
 
 
-def _content(perm: tuple[int, ...], flips: tuple[int, ...]) -> int:
-    return PRANK[perm] * 16 + sum(f << i for i, f in enumerate(flips))
+def _symmetry_actions() -> list[np.ndarray]:
+    """The relabellings of the E cubies (8..11) induced by the 16 U-D symmetries, as content maps."""
+
+    return [relabel_action([int(es.perm[8 + x]) - 8 for x in range(4)], [int(es.flip[8 + x]) for x in range(4)])
+            for es in coords.ud_actions()[1]]
+
+
+def _orbits(actions: list[np.ndarray]) -> np.ndarray:
+    """Orbit id of every content under the group the content maps generate, the orbits numbered
+    by their smallest content.  Union-find over the generators' edges: the group is finite, so
+    closing under the generators closes under the group."""
+
+    root = np.arange(N_CONTENT)
+
+    def find(x: int) -> int:
+        while root[x] != x:
+            root[x] = root[root[x]]
+            x = root[x]
+        return x
+
+    for a in actions:
+        for c in range(N_CONTENT):
+            u, v = find(c), find(int(a[c]))
+            if u != v:
+                root[max(u, v)] = min(u, v)  # the smaller content stays the root
+    roots = np.array([find(c) for c in range(N_CONTENT)])
+    minima = np.unique(roots)  # sorted: orbit ids follow the orbit minima
+    return np.searchsorted(minima, roots)
 
 
 class GroupKind:
-    """Edge factor: non-E flips (256) x E content (384) up to the group L.
+    """Edge factor: non-E flips (256) x E content (384) up to a relabelling group L <= B4.
 
     ``gen = (gen_class[384], gen_rep[2, 384])``: the class of every content (order rank * 16 +
-    flips by position), and a representative content per class for each E-flip parity.
+    flips by position), and a representative content per class for each E-flip parity.  L is
+    given by generators; it acts on contents by relabelling, and its classes are the orbits of
+    that action.
     """
 
     ep = 9
@@ -75,38 +91,43 @@ class GroupKind:
     def __init__(self, name: str, gens):
         self.name = name
         self.gens_list = [(tuple(p), tuple(f)) for p, f in gens]
-        self.group = _closure(self.gens_list)
-        if any(_mul(_mul(s, x), _inverse(s)) not in self.group for s in _sym_image() for x in self.group):
-            raise ValueError(f"{name}: group not normalised by the UD symmetries; symmetry reduction would be wrong")
-        cls = np.full(384, -1, dtype=np.int64)
-        reps: list[int] = []
-        for c in range(384):  # classes numbered in order of their smallest content
-            if cls[c] >= 0:
-                continue
-            q, g = PERMS[c // 16], [(c >> i) & 1 for i in range(4)]
-            for kp, kf in self.group:
-                cls[_content(tuple(kp[q[i]] for i in range(4)), tuple(g[i] ^ kf[q[i]] for i in range(4)))] = len(reps)
-            reps.append(c)
-        parity = np.array([bin(c & 15).count("1") & 1 for c in range(384)])
-        gen_class = np.zeros(384, np.uint16)
-        gen_rep = np.zeros((2, 384), np.uint16)
-        if all(sum(f) % 2 == 0 for _, f in self.group):
-            # Every relabelling keeps the E-flip parity, which the non-E flips then determine:
-            # number the classes within each parity.
-            within = []
-            count = [0, 0]
-            for r in reps:
-                p = parity[r]
-                within.append(count[p])
-                gen_rep[p, count[p]] = r
-                count[p] += 1
-            self.nec = len(reps) // 2
-            gen_class[:] = [within[cls[c]] for c in range(384)]
+        actions = [relabel_action(p, f) for p, f in self.gens_list]
+        orbit = _orbits(actions)
+        # Symmetry reduction conjugates the content by a U-D symmetry's relabelling s; that is only
+        # well defined if s carries L-orbits onto L-orbits (s L s^-1 = L: the orbits are L's right
+        # cosets, and a subgroup is the coset of the identity).  Orbits are closed under the
+        # generators, so it suffices that s(c) and s(g(c)) share an orbit for every generator g.
+        for s in _symmetry_actions():
+            for a in actions:
+                if not np.array_equal(orbit[s], orbit[s[a]]):
+                    raise ValueError(f"{name}: group not normalised by the UD symmetries; symmetry reduction would be wrong")
+        parity = _FLIPS.sum(axis=1) & 1
+        n_orbits = int(orbit.max()) + 1
+        gen_class = np.zeros(N_CONTENT, np.uint16)
+        gen_rep = np.zeros((2, N_CONTENT), np.uint16)
+        keeps_parity = all(sum(f) % 2 == 0 for _, f in self.gens_list)
+        if keeps_parity:
+            # Every relabelling keeps the E-flip parity, which the non-E flips then determine: the
+            # classes are numbered within each parity (in order of their smallest content), and a
+            # class's representative is its smallest content.
+            orbit_parity = np.zeros(n_orbits, np.int64)
+            orbit_parity[orbit] = parity
+            rank = np.zeros(n_orbits, np.int64)
+            for p in (0, 1):
+                ids = np.flatnonzero(orbit_parity == p)
+                rank[ids] = np.arange(len(ids))
+                first = np.array([np.flatnonzero(orbit == i)[0] for i in ids], dtype=np.int64)
+                gen_rep[p, : len(ids)] = first
+            gen_class[:] = rank[orbit]
+            self.nec = n_orbits // 2
         else:
-            self.nec = len(reps)
-            gen_class[:] = cls
-            for c in range(384):
-                gen_rep[parity[c], cls[c]] = c
+            # Classes hold both parities: per parity, a class's representative is its largest
+            # content of that parity.
+            gen_class[:] = orbit
+            for p in (0, 1):
+                sel = np.flatnonzero(parity == p)
+                gen_rep[p, orbit[sel]] = sel  # ascending contents: the last write is the largest
+            self.nec = n_orbits
         self.n_edge = coords.N_SLICE * 256 * self.nec
         self.defines = ("EDGE_EP=9", "EDGE_EO=1", f"GEN_NEC={self.nec}")
         self.gen = (gen_class, gen_rep)
@@ -190,10 +211,12 @@ class Preset:
 
     @property
     def build_bytes(self) -> int:
-        """Device memory the reference needs to build it (mod-3 table plus block table); kept as
-        the ladder's rule so ``choose`` picks the same preset as the reference."""
+        """Peak device memory of building it here: one exact-depth byte per entry (padded to 16)
+        and the encoded block table, plus the base-3 table while it is encoded from the block one."""
 
-        return (self.entries + 15) // 16 * 4 + -(-self.entries // BLOCK_ENTRIES) * 32
+        depth = -(-self.entries // 16) * 16
+        block = -(-self.entries // BLOCK_ENTRIES) * 32
+        return depth + block + (self.table_bytes if self.format == "b3" else 0)
 
 
 # The memory ladder, smallest first: each step is faster on random cubes and bigger.
@@ -224,17 +247,19 @@ def built(preset: Preset, tables: Path) -> bool:
 
 def choose(tables: Path, memory: int, build_memory: int | None = None,
            to_build: bool = False) -> tuple[Preset | None, Preset | None]:
-    """The fastest preset whose table fits in ``memory`` bytes and is built or can be built (in
-    ``build_memory``, default ``memory``), and the fastest that would fit but can't be built
-    here (None if that is no faster).  ``to_build``: ignore tables already built."""
+    """The fastest preset whose table fits in ``memory`` bytes and is either built already or can
+    be built in ``build_memory`` bytes (default ``memory``); and, when a faster one would fit but
+    can't be built here, that one (else None).  ``to_build``: tables already built don't count."""
 
     build_memory = memory if build_memory is None else build_memory
-    fits = [p for p in PRESETS if p.auto and p.table_bytes + SOLVE_MARGIN <= memory]
-    usable = [p for p in fits
-              if (built(p, tables) and not to_build) or p.build_bytes + SOLVE_MARGIN <= build_memory]
-    best = usable[-1] if usable else None
-    better = fits[-1] if fits and fits[-1] is not best else None
-    return best, better
+    blocked = None
+    for p in reversed([q for q in PRESETS if q.auto]):  # fastest first
+        if p.table_bytes + SOLVE_MARGIN > memory:
+            continue
+        if (not to_build and built(p, tables)) or p.build_bytes + SOLVE_MARGIN <= build_memory:
+            return p, blocked
+        blocked = blocked or p
+    return None, blocked
 
 
 def free_device_memory() -> int:
@@ -260,14 +285,19 @@ def pick(tables: Path, memory="auto", name: str | None = None,
 
 
 def describe(tables: Path) -> list[str]:
-    rows = [f"{'preset':8} {'VRAM':>8} {'cubes/s':>8} {'superflip':>10} {'build VRAM':>11}  file"]
+    """The preset table of ``cuda-cube-solver tables``: size, speed, build memory, file status."""
+
+    head = f"{'preset':8} {'VRAM':>8} {'cubes/s':>8} {'superflip':>10} {'build VRAM':>11}  file"
+    rows = [head]
     for p in PRESETS:
+        notes = ("" if built(p, tables) else "  (not built)") + ("" if p.auto else "  (only with --table)")
         rows.append(f"{p.name:8} {p.table_bytes / 1e9:6.2f}GB {p.cubes_per_s:8.1f} {p.superflip_s:9.1f}s "
-                    f"{p.build_bytes / 1e9:9.1f}GB  {p.file}{'' if built(p, tables) else '  (not built)'}"
-                    f"{'' if p.auto else '  (only with --table)'}")
+                    f"{p.build_bytes / 1e9:9.1f}GB  {p.file}{notes}")
     return rows
 
 
 def write_meta(path: Path, preset: Preset, counts: list[int], seconds: float) -> None:
-    Path(path).write_text(json.dumps({"preset": preset.name, "entries": preset.entries, "depth_counts": counts,
-                                      "seconds": round(seconds, 1)}, indent=2) + "\n")
+    """The ``.json`` beside a table file: preset, entries, per-depth counts, build seconds."""
+
+    meta = {"preset": preset.name, "entries": preset.entries, "depth_counts": counts, "seconds": round(seconds, 1)}
+    Path(path).write_text(json.dumps(meta, indent=2) + "\n")

@@ -114,11 +114,24 @@ class GpuSolver:
     """
 
     def __init__(self, tables: Path = Path("tables"), prefix_len: int = 4, grid: int | None = None, block: int = 256,
-                 inverse: bool = True, collect_stats: bool = False, mode: str = "step", table_format: str = "block",
-                 kind="d4t", deeper_prefix_at: tuple[float, ...] = (5e7, 3e9), handle: native.Handle | None = None,
-                 device: int = 0):
+                 inverse: bool = True, collect_stats: bool = False, mode: str = "step",
+                 extra_tables: int = 2, step_extra: int = 0, table_format: str = "block",
+                 step_defines: tuple[str, ...] = (), kind="d4t",
+                 deeper_prefix_at: tuple[float, ...] = (5e7, 3e9), extra_kind=None,
+                 handle: native.Handle | None = None, device: int = 0):
+        # The reference's keywords (solver.py:119-123) are all accepted; those of its experimental
+        # search modes (extra tables, extra kinds, NVRTC defines) are not built and are refused
+        # with ValueError like the reference refuses invalid combinations (solver.py:145-148).
+        # ``extra_tables`` only matters for mode="multi", which is refused below.
         if mode != "step" or not inverse:
             raise ValueError("only the step search with inverse frames is built (mode='step', inverse=True)")
+        if step_extra:
+            raise ValueError("step_extra tables (208 + 112/304 lookups) are not built; use a kind preset")
+        if step_defines:
+            raise ValueError("step_defines (NVRTC kernel defines) do not apply: the kernels are compiled for sm_100a")
+        if extra_kind is not None:
+            raise ValueError("extra_kind (a second lookup table per node) is not built; attach_second() keeps a "
+                             "second table resident and picks one per cube")
         tables = Path(tables)
         if tables.suffix == ".bin":
             tables = tables.parent

@@ -152,9 +152,11 @@ int ccs_solve_tables(ccs_handle* h, const uint32_t* states, const uint8_t* table
  * at start-up.  No counterpart in the reference.  The search buffers are one fixed array in the
  * library's device image (304 KB on every GPU that loads the library); at most
  * CCS_NOALLOC_MAX_CUBES cubes per call, prefixes of at most 4 moves (opts->base_plen <= 4;
- * deeper_at0/1 are ignored), the first table only.  The first call on a device sets the array up
- * (with that device current) and should come before any stream capture.  One array per process
- * and device: calls that overlap on the GPU race on it. */
+ * deeper_at0/1 are ignored), the first table only, devices 0..15.  The first call on a device sets
+ * the array up (with that device current) and should come before any stream capture; a call after
+ * a device reset sets it up again.  One array per process and device, shared by every handle on
+ * that device: calls on one device would race on it, so the library runs them one at a time (a
+ * per-device lock; calls on different devices do not wait for each other). */
 #define CCS_NOALLOC_MAX_CUBES 256
 int ccs_solve_noalloc(ccs_handle* h, const uint32_t* states, int n, const ccs_solve_opts* opts,
                       ccs_result* results);

@@ -120,3 +120,18 @@ def test_server_picks_the_second_table_by_the_flip_rule():
     srv.submit(workloads.superflip())
     srv.close()
     assert plain.submits[0][1] == 0 and h.started is None
+
+
+def test_gpusolver_refuses_unbuilt_reference_keywords():
+    """The reference's GpuSolver keywords are accepted; those of its experimental search modes
+    raise ValueError before any device work (as the reference does for invalid combinations)."""
+
+    import pytest
+
+    from cuda_cube_solver.solver import GpuSolver
+
+    for kw, match in (({"mode": "multi"}, "mode='step'"), ({"inverse": False}, "mode='step'"),
+                      ({"step_extra": 1}, "step_extra"), ({"step_defines": ("-DX",)}, "step_defines"),
+                      ({"extra_kind": "s4"}, "extra_kind")):
+        with pytest.raises(ValueError, match=match):
+            GpuSolver(**kw)

@@ -125,11 +125,15 @@ def test_group_kind_roundtrip_and_cosets(name):
         assert int(kind.edge_coord(kind.edges_from_coord(coord))) == coord
 
     def relabel(state):
-        kp, kf = rng.choice(sorted(kind.group))
+        # a random group element: a random word in the generators, applied one letter at a time
         others = list(range(8))
         rng.shuffle(others)
-        ep = tuple(8 + kp[c - 8] if c >= 8 else others[c] for c in state.ep)
-        eo = tuple(o ^ kf[c - 8] if c >= 8 else o for c, o in zip(state.ep, state.eo))
+        ep = tuple(c if c >= 8 else others[c] for c in state.ep)
+        eo = state.eo
+        for _ in range(rng.randrange(1, 6)):
+            kp, kf = rng.choice(kind.gens_list)
+            eo = tuple(o ^ kf[c - 8] if c >= 8 else o for c, o in zip(ep, eo))
+            ep = tuple(8 + kp[c - 8] if c >= 8 else c for c in ep)
         return CubieState(state.cp, state.co, ep, eo)
 
     for state in _random_states(15, 17):
@@ -142,13 +146,16 @@ def test_group_kind_roundtrip_and_cosets(name):
 
 def test_preset_choice(tmp_path):
     names = lambda pair: tuple(p.name if p else None for p in pair)  # noqa: E731
-    assert names(kinds.choose(tmp_path, int(16e9))) == ("d4t", None)
-    assert names(kinds.choose(tmp_path, int(8e9), int(16e9))) == ("d4t-b3", None)
-    assert names(kinds.choose(tmp_path, int(8e9))) == ("s4-b3", "d4t-b3")
+    # a 16 GB budget on a GPU with 180 GB free: the d4t build (38 GB) fits beside it
+    assert names(kinds.choose(tmp_path, int(16e9), int(180e9))) == ("d4t", None)
+    assert names(kinds.choose(tmp_path, int(8e9), int(180e9))) == ("d4t-b3", None)
+    # on a 16 GB GPU the d4t table would fit but its build does not: s4-b3 (14.7 GB to build)
+    assert names(kinds.choose(tmp_path, int(16e9))) == ("s4-b3", "d4t")
+    assert names(kinds.choose(tmp_path, int(8e9))) == ("304", "d4t-b3")
     (tmp_path / "prune-ud-d4t-b3.bin").touch()
     assert names(kinds.choose(tmp_path, int(8e9))) == ("d4t-b3", None)
     assert names(kinds.choose(tmp_path, int(1e9))) == (None, None)
-    assert names(kinds.choose(tmp_path, int(8e9), to_build=True)) == ("s4-b3", "d4t-b3")
+    assert names(kinds.choose(tmp_path, int(8e9), to_build=True)) == ("304", "d4t-b3")
 
 
 def test_preset_sizes():
@@ -157,7 +164,9 @@ def test_preset_sizes():
     assert by["d4t"].table_bytes == 7_793_525_280
     assert by["d4t-b3"].table_bytes == 6_234_820_224
     assert by["304"].table_bytes == 1_420_694_720
-    assert by["d4t"].build_bytes == 15_343_502_880
+    # this library's build: 30,199,910,400 depth bytes + the 7,793,525,280-byte block table
+    assert by["d4t"].build_bytes == 30_199_910_400 + 7_793_525_280
+    assert by["d4t-b3"].build_bytes == 30_199_910_400 + 7_793_525_280 + 6_234_820_224
 
 
 def test_group_kind_must_be_normalised_by_the_symmetries():

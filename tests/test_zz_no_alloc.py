@@ -54,3 +54,48 @@ def test_no_alloc_full_batch_and_limits(lengths_golden):
     with pytest.raises(native.CcsError, match="base_plen 5"):
         h.solve_noalloc(words[:1], native.solve_opts(base_plen=5))
     assert h.solve_noalloc(words[:0]) == []
+
+
+def test_no_alloc_prefix_length_one_many_cubes(lengths_golden):
+    """base_plen = 1 with 32 or more cubes in flight: the shallow rule takes the next iteration's
+    prefix length below 1, which is clamped to 1 (a wrapped length would ask for prefix lists the
+    array does not hold and stall the search).  The allocating path gives the same lengths."""
+
+    h = resident_handle("d4t")
+    cubes = lengths_golden["random1000"][500:540]
+    words = _words(cubes)
+    opts = native.solve_opts(base_plen=1, timeout_s=600)
+    got = h.solve_noalloc(words, opts)
+    ref = h.solve(words, opts)
+    assert [r.length for r in got] == [r.length for r in ref] == [c["length"] for c in cubes]
+    assert verify_solutions(words, [list(r.moves[: r.length]) for r in got])
+
+
+def test_no_alloc_two_threads_one_device(lengths_golden):
+    """Two handles on one device (d4t and 304 tables) share its array; the library runs their calls
+    one at a time, so two threads calling together both get their own cubes' results."""
+
+    import threading
+
+    from cuda_cube_solver import workloads
+
+    h1 = resident_handle("d4t")
+    h2 = resident_handle("304")
+    w1 = _words(lengths_golden["random1000"][600:630])
+    w2 = state_words([workloads.scramble_state(s) for s in workloads.small_scrambles(40, seed=7)])
+    opts = native.solve_opts(timeout_s=600)
+    want = [[r.length for r in h1.solve(w1, opts)], [r.length for r in h2.solve(w2, opts)]]
+    out = [None, None]
+
+    def run(i, h, w):
+        out[i] = h.solve_noalloc(w, opts)
+
+    for _ in range(2):
+        threads = [threading.Thread(target=run, args=(0, h1, w1)), threading.Thread(target=run, args=(1, h2, w2))]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        for i, w in enumerate((w1, w2)):
+            assert [r.length for r in out[i]] == want[i]
+            assert verify_solutions(w, [list(r.moves[: r.length]) for r in out[i]])
