@@ -90,16 +90,20 @@ struct ccs_handle {
     ccs::QueueState* d_q = nullptr;
     unsigned long long* d_ring = nullptr;
     uint32_t ring_cap = 0;
+    ccs::DonationCell* d_don = nullptr;  // work-stealing cells (ccs::DON_CELLS)
     uint32_t* d_prefix[ccs::MAX_PLEN + 1] = {};
     uint32_t n_prefix[ccs::MAX_PLEN + 1] = {};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_kernel_ms = 0;
     uint64_t last_probes = 0;
+    uint64_t last_donated = 0;
+    uint64_t last_h2d = 0, last_d2h = 0;
     int last_launches = 0;
     ccs::Server* server = nullptr;
 };
 
 namespace ccs {
+constexpr uint32_t DON_CELLS = 4096;  // donation cells of a handle's search buffers (128 KB)
 int set_kind(ccs_handle* h, const char* name);
 void free_table(ccs_handle* h);
 int ensure_search_buffers(ccs_handle* h, uint32_t slots);

@@ -212,6 +212,7 @@ int ccs_close(ccs_handle* h) {
     cudaFree(h->d_slots);
     cudaFree(h->d_q);
     cudaFree(h->d_ring);
+    cudaFree(h->d_don);
     for (auto* p : h->d_prefix) cudaFree(p);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);

@@ -1,0 +1,6 @@
+// Search kernels of group kinds of 16 E-content classes (a4t, a4).
+#include "search_launch.cuh"
+
+namespace ccs {
+template int launch_kind<KIND_GEN, 16>(ccs_handle*, const SearchParams&, int, cudaStream_t, int);
+}  // namespace ccs

@@ -1,0 +1,6 @@
+// Search kernels of group kinds of 8 E-content classes (s4).
+#include "search_launch.cuh"
+
+namespace ccs {
+template int launch_kind<KIND_GEN, 8>(ccs_handle*, const SearchParams&, int, cudaStream_t, int);
+}  // namespace ccs

@@ -176,6 +176,8 @@ extern "C" int ccs_solve_noalloc(ccs_handle* h, const uint32_t* states, int n, c
     // every iteration stays at or below the base prefix length: no longer lists exist here
     P.deeper_at[0] = P.deeper_at[1] = ~0ull;
     P.max_plen = NOALLOC_MAX_PLEN;
+    P.don = nullptr;  // no work stealing: its cells would be one more buffer
+    P.don_cap = 0;
 
     // The array keeps the previous call's contents: the slots of this call, the queue state and
     // both rings are rewritten before the launch.

@@ -24,7 +24,9 @@ struct alignas(16) Slot {
     uint32_t h0;                     // root lower bounds, 5 bits per frame
     uint32_t status;
     unsigned long long ticket;
-    uint32_t done;                   // items finished in the current epoch
+    uint32_t open;                   // work units of the current epoch not yet finished: its items,
+                                     // plus subtrees donated by lanes still holding a unit (so it
+                                     // reaches 0 exactly when the epoch's last unit finishes)
     uint32_t found;                  // set by the first lane that finds a solution
     uint32_t sol_len;
     uint32_t request;                // caller's tag (server request id)
@@ -48,8 +50,22 @@ struct QueueState {
     unsigned long long admit_head;   // admission ring: cubes waiting for a first iteration
     unsigned long long admit_tail;
     uint32_t yield;                  // host asks lanes to stop fetching new items
+    uint32_t starving;               // set by a lane that found no item and no donated subtree
+    unsigned long long donated;      // subtrees donated (diagnostic)
+    uint32_t don_count;              // donated subtrees waiting in the donation cells
     uint32_t pad;
 };
+
+// A donated subtree: the unexplored children of one node of a running item (the node at depth g0
+// on the donor's path), handed to an idle lane.  Cell state: 0 empty, 1 being written, 2 full,
+// 3 being read.  Payload: w1 = h of the node (30 bits) | g0 << 32 | bound << 37 | todo << 42;
+// w2 / w3 = the path to the node, 5 bits per move (moves 0..11, 12..23).
+struct alignas(32) DonationCell {
+    uint32_t state;
+    uint32_t slot;
+    unsigned long long w1, w2, w3;
+};
+constexpr uint32_t DON_EMPTY = 0, DON_WRITING = 1, DON_FULL = 2, DON_READING = 3;
 
 constexpr uint32_t ERR_IDLE_LIMIT = 1u, ERR_BOUND = 2u, ERR_STACK = 4u;
 
@@ -78,6 +94,11 @@ struct SearchParams {
     uint32_t move_min;               // phased kernel: lanes waiting before a MOVE pass runs
     uint32_t move_age;               // phased kernel: iterations a waiting lane may be deferred
     uint32_t probe_min;              // phased kernel: probe pass repeats while this many lanes probe
+    DonationCell* don;               // donation cells (null: no work stealing)
+    uint32_t don_cap;                // number of cells
+    uint32_t don_target;             // donors stop once this many subtrees wait
+    uint32_t don_min_depth;          // a donated node has at least this many moves left to the bound
+    uint32_t don_period;             // a lane with work checks for starving lanes every this many iterations
     uint32_t persistent;             // server: an empty queue is not the end (lanes wait for new cubes)
     unsigned long long* done_log;    // host-mapped completion log (server), may be null
     uint32_t done_log_cap;

@@ -111,7 +111,7 @@ __device__ __forceinline__ bool ticket_open(const SearchParams& P, unsigned long
 __device__ __forceinline__ void publish_epoch(const SearchParams& P, uint32_t s, uint32_t plen, uint32_t bound,
                                               uint32_t epoch) {
     Slot& sl = P.slots[s];
-    sl.done = 0;
+    sl.open = P.n_prefix[plen];
     __threadfence();
     atomicExch(&sl.ticket, ticket_make(plen, bound, epoch));
     __threadfence();
@@ -158,6 +158,62 @@ __device__ __forceinline__ uint32_t next_plen(const SearchParams& P, unsigned lo
     const int top = (int)P.max_plen;  // the longest prefix length with a list in this launch
     pl = pl < 1 ? 1 : (pl > top ? top : pl);
     return (uint32_t)pl < bound ? (uint32_t)pl : bound;
+}
+
+// A lane finished a work unit (an item or a donated subtree) of slot s's current epoch: true for
+// the lane that finished its last one.
+__device__ __forceinline__ bool finish_unit(const SearchParams& P, uint32_t s) {
+    __threadfence();
+    const bool last = atomicSub(&P.slots[s].open, 1u) == 1u;
+    if (last) __threadfence();
+    return last;
+}
+
+// Work stealing.  A lane whose item still has unexplored children at a shallow node of its path
+// donates them when lanes starve: the node's depth, bounds, path and remaining children go into
+// a free donation cell, the epoch's open count grows by one first (the donor still holds its own
+// unit, so the count cannot reach zero meanwhile), and the donor skips those children.  An idle
+// lane takes a cell, replays the path on the root frames and searches the children as a unit of
+// its own, which it may split again.  Cells are claimed with compare-and-swap on their state and
+// scanned a bounded number of times; nothing waits.
+__device__ __forceinline__ bool post_donation(const SearchParams& P, uint32_t seed, uint32_t slot,
+                                              unsigned long long w1, unsigned long long w2, unsigned long long w3) {
+    for (uint32_t i = 0; i < 32u; ++i) {
+        DonationCell& cell = P.don[(seed + i) % P.don_cap];
+        if (*(volatile uint32_t*)&cell.state != DON_EMPTY) continue;
+        if (atomicCAS(&cell.state, DON_EMPTY, DON_WRITING) != DON_EMPTY) continue;
+        cell.slot = slot;
+        cell.w1 = w1;
+        cell.w2 = w2;
+        cell.w3 = w3;
+        __threadfence();
+        atomicExch(&cell.state, DON_FULL);
+        atomicAdd(&P.q->don_count, 1u);
+        atomicAdd(&P.q->donated, 1ull);
+        return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ bool take_donation(const SearchParams& P, uint32_t seed, uint32_t& slot,
+                                              unsigned long long& w1, unsigned long long& w2,
+                                              unsigned long long& w3) {
+    if ((int)*(volatile uint32_t*)&P.q->don_count <= 0) return false;
+    for (uint32_t i = 0; i < 64u; ++i) {
+        DonationCell& cell = P.don[(seed + i) % P.don_cap];
+        if (*(volatile uint32_t*)&cell.state != DON_FULL) continue;
+        if (atomicCAS(&cell.state, DON_FULL, DON_READING) != DON_FULL) continue;
+        __threadfence();
+        slot = *(volatile uint32_t*)&cell.slot;
+        w1 = *(volatile unsigned long long*)&cell.w1;
+        w2 = *(volatile unsigned long long*)&cell.w2;
+        w3 = *(volatile unsigned long long*)&cell.w3;
+        __threadfence();
+        atomicExch(&cell.state, DON_EMPTY);
+        atomicSub(&P.q->don_count, 1u);
+        return true;
+    }
+    return false;
 }
 
 enum FetchResult { FETCH_OK = 0, FETCH_EMPTY = 1, FETCH_FINISHED = 2, FETCH_ADMIT = 3 };
@@ -455,9 +511,7 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel(const DevTables* 
                 }
                 Slot& sl = P.slots[slot];
                 if (*(volatile uint32_t*)&sl.found) {  // solved by another item: skip
-                    __threadfence();
-                    uint32_t d = atomicAdd(&sl.done, 1u) + 1u;
-                    if (d == P.n_prefix[plen]) finish_slot(P, slot, SLOT_SOLVED);
+                    if (finish_unit(P, slot)) finish_slot(P, slot, SLOT_SOLVED);
                     continue;
                 }
 f.load(sl.frame);
@@ -494,10 +548,7 @@ f.load(sl.frame);
                 atomicAdd(&sl.probes, probes);
                 atomicAdd(&sl.iter_nodes[bound < 24u ? bound : 23u], nodes);
                 atomicAdd(&P.q->probes, probes);
-                __threadfence();
-                uint32_t d = atomicAdd(&sl.done, 1u) + 1u;
-                if (d == P.n_prefix[plen]) {
-                    __threadfence();
+                if (finish_unit(P, slot)) {
                     if (*(volatile uint32_t*)&sl.found) {
                         finish_slot(P, slot, SLOT_SOLVED);
                     } else if (bound + 1u > MAX_BOUND) {

@@ -35,6 +35,12 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lane_seed = (blockIdx.x * blockDim.x + threadIdx.x) * 0x9E3779B1u >> 7;
 
+    // Work stealing (not with LOOKAHEAD, whose stash holds siblings the donation would repeat):
+    // gbase = depth of the lane's unit root (0 for an item, the donated node's depth for a donated
+    // subtree); bit l of `cut` = the remaining children of the node at depth l were donated.
+    constexpr bool STEAL = !LOOKAHEAD;
+    int gbase = 0;
+    uint32_t cut = 0, don_tick = 0;
     int mv = 0;  // frame update this lane waits for: 0 none, 1 push child m, 2 pop one level
     // LOOKAHEAD: the next sibling of the child under evaluation, evaluated alongside it; when the
     // child is pushed, the sibling's partial evaluation waits in a per-level stash (bit g of
@@ -70,8 +76,8 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                 m2 = -1;
             }
         }
-        // A node with no children left pops one level.
-        if (have && m < 0 && todo == 0u && g > 0 && mv == 0) mv = 2;
+        // A node with no children left pops one level (a unit ends at its root depth).
+        if (have && m < 0 && todo == 0u && g > gbase && mv == 0) mv = 2;
         // MOVE: push and pop both apply a move to all six frames (pop with the inverse moves), so
         // one pass serves every waiting lane; it runs once enough lanes wait, after a few
         // iterations, or when no lane could probe meanwhile.
@@ -119,6 +125,10 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                                    ~((2u << mm) - 1u);
                             ord = frame_order(h, bound - (uint32_t)g);
                         }
+                        if (STEAL && ((cut >> g) & 1u)) {  // this node's remaining children were donated
+                            todo = 0u;
+                            cut &= ~(1u << g);
+                        }
                         if (LOOKAHEAD && ((stash >> g) & 1u)) {  // the stashed sibling resumes
                             stash &= ~(1u << g);
                             const uint32_t x = la_x[g];
@@ -137,22 +147,21 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
         if (have && mv == 0 && (++iter & 255u) == 0u &&
             (*(volatile uint32_t*)&P.slots[slot].found || ((volatile QueueState*)P.q)->yield)) {
             todo = 0u;
-            g = 0;
+            g = gbase;  // (the frames are reloaded with the next unit)
             m = -1;
             m2 = -1;
             stash = 0u;
         }
-        // FINISH the item; the lane finishing an iteration's last item closes the iteration.
-        if (have && mv == 0 && m < 0 && todo == 0u && g == 0) {
+        // FINISH the unit; the lane finishing an iteration's last unit closes the iteration.
+        if (have && mv == 0 && m < 0 && todo == 0u && g == gbase) {
             Slot& sl = P.slots[slot];
             atomicAdd(&sl.nodes, (unsigned long long)nodes);
             atomicAdd(&sl.probes, (unsigned long long)probes);
             atomicAdd(&sl.iter_nodes[bound < 24u ? bound : 23u], (unsigned long long)nodes);
             atomicAdd(&P.q->probes, (unsigned long long)probes);
-            __threadfence();
-            uint32_t d = atomicAdd(&sl.done, 1u) + 1u;
-            if (d == P.n_prefix[plen]) {
-                __threadfence();
+            gbase = 0;
+            cut = 0u;
+            if (finish_unit(P, slot)) {
                 if (*(volatile uint32_t*)&sl.found) {
                     finish_slot(P, slot, SLOT_SOLVED);
                 } else if (bound + 1u > MAX_BOUND) {
@@ -169,7 +178,18 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
         if (!have && !done && fetch_wait) {
             --fetch_wait;  // the queue was empty: retry in a few iterations, not on every one
         } else if (!have && !done) {
-            int r = fetch_item(P, lane_seed + (fetches++) * 0x2545F491u, slot, idx, plen, bound, epoch);
+            const uint32_t seed = lane_seed + (fetches++) * 0x2545F491u;
+            int r = fetch_item(P, seed, slot, idx, plen, bound, epoch);
+            unsigned long long w1 = 0, w2 = 0, w3 = 0;
+            bool donated_unit = false;
+            if (STEAL && r == FETCH_EMPTY && P.don_cap) {
+                donated_unit = take_donation(P, seed, slot, w1, w2, w3);
+                if (donated_unit) {
+                    r = FETCH_OK;
+                } else if (!*(volatile uint32_t*)&P.q->starving) {
+                    *(volatile uint32_t*)&P.q->starving = 1u;  // no item, no subtree: ask for donations
+                }
+            }
             if (r == FETCH_EMPTY) fetch_wait = 16;
             if (r == FETCH_FINISHED) {
                 done = true;
@@ -177,10 +197,37 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                 admit_slot<MODE, NEC, FMT>(T, P, slot);
             } else if (r == FETCH_OK) {
                 Slot& sl = P.slots[slot];
-                if (*(volatile uint32_t*)&sl.found) {  // solved by another item: count it done
-                    __threadfence();
-                    uint32_t d = atomicAdd(&sl.done, 1u) + 1u;
-                    if (d == P.n_prefix[plen]) finish_slot(P, slot, SLOT_SOLVED);
+                if (*(volatile uint32_t*)&sl.found) {  // solved by another unit: count it done
+                    if (finish_unit(P, slot)) finish_slot(P, slot, SLOT_SOLVED);
+                } else if (STEAL && donated_unit && (((w1 >> 32) & 31u) >= (uint32_t)MAX_DEPTH ||
+                                                      ((w1 >> 37) & 31u) > MAX_BOUND)) {
+                    atomicOr(&P.q->error, ERR_STACK);  // a malformed cell (never written by a donor)
+                    if (finish_unit(P, slot)) finish_slot(P, slot, SLOT_ERROR);
+                } else if (STEAL && donated_unit) {
+                    // a donated subtree: the node at depth g0 on the donor's path, its bounds and
+                    // remaining children; the frames are the root's with the path replayed
+                    const int g0 = (int)((w1 >> 32) & 31u);
+                    bound = (uint32_t)((w1 >> 37) & 31u);
+                    epoch = (uint32_t)(*(volatile unsigned long long*)&sl.ticket >> 32) & 0xFFFFu;
+                    f.load(sl.frame);
+                    for (int j = 0; j < g0; ++j) {
+                        const int mj = (int)(((j < 12 ? w2 : w3) >> (5 * (j % 12))) & 31u);
+                        path[j] = (unsigned char)mj;
+                        f.step(T, mj);
+                    }
+                    second = sl.table != 0u;
+                    h = (uint32_t)w1 & 0x3FFFFFFFu;
+                    g = gbase = g0;
+                    plen = 0;
+                    pseq = 0;
+                    nodes = 0;
+                    probes = 0;
+                    cut = 0u;
+                    stash = 0u;
+                    m2 = -1;
+                    todo = (uint32_t)(w1 >> 42) & 0x3FFFFu;
+                    ord = frame_order(h, bound - (uint32_t)g0);
+                    have = true;
                 } else {
                     f.load(sl.frame);
                     second = sl.table != 0u;
@@ -195,6 +242,47 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                     todo = allow & ~axis_move_mask(excluded_axes(h, bound));
                     ord = frame_order(h, bound);
                     have = true;
+                }
+            }
+        }
+        // DONATE: while lanes starve, hand the remaining children of the shallowest node on this
+        // lane's path that still has some (and enough depth left to be worth a replay) to them.
+        if (STEAL && P.don_cap && have && mv == 0 && (++don_tick & (P.don_period - 1u)) == 0u &&
+            *(volatile uint32_t*)&P.q->starving) {
+            volatile QueueState* q = P.q;
+            if ((int)q->don_count >= (int)P.don_target) {
+                q->starving = 0u;
+            } else {
+                const int lo = gbase > (int)plen ? gbase : (int)plen;
+                for (int l = lo; l <= g; ++l) {
+                    if (bound < (uint32_t)l + P.don_min_depth) break;
+                    uint32_t rest, hl;
+                    if (l == g) {
+                        rest = todo;
+                        hl = h;
+                    } else {
+                        if ((cut >> l) & 1u) continue;
+                        hl = hstack[l];
+                        const int last = l > 0 ? path[l - 1] : -1;
+                        rest = T.amask[last + 1] & ~axis_move_mask(excluded_axes(hl, bound - (uint32_t)l)) &
+                               ~((2u << path[l]) - 1u);
+                    }
+                    if (!rest) continue;
+                    unsigned long long w2 = 0, w3 = 0;
+                    for (int j = 0; j < l; ++j) {
+                        if (j < 12) w2 |= (unsigned long long)path[j] << (5 * j);
+                        else w3 |= (unsigned long long)path[j] << (5 * (j - 12));
+                    }
+                    const unsigned long long w1 = (unsigned long long)hl | ((unsigned long long)l << 32) |
+                                                  ((unsigned long long)bound << 37) | ((unsigned long long)rest << 42);
+                    atomicAdd(&P.slots[slot].open, 1u);  // before the post: the count never runs short
+                    if (post_donation(P, lane_seed + don_tick, slot, w1, w2, w3)) {
+                        if (l == g) todo = 0u;
+                        else cut |= 1u << l;
+                    } else {
+                        atomicSub(&P.slots[slot].open, 1u);  // (this lane's own unit keeps it above 0)
+                    }
+                    break;
                 }
             }
         }

@@ -194,6 +194,7 @@ extern "C" int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* 
     QueueState q;
     std::memset(&q, 0, sizeof q);
     CCS_CUDA_TRY(cudaMemsetAsync(h->d_ring, 0xFF, sizeof(unsigned long long) * (h->ring_cap + h->slot_cap), s->copy));
+    CCS_CUDA_TRY(cudaMemsetAsync(h->d_don, 0, sizeof(DonationCell) * DON_CELLS, s->copy));
     CCS_CUDA_TRY(cudaMemcpyAsync(h->d_q, &q, sizeof q, cudaMemcpyHostToDevice, s->copy));
     CCS_CUDA_TRY(cudaStreamSynchronize(s->copy));
     s->slot_request.assign(h->slot_cap, 0);

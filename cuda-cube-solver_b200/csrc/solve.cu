@@ -8,13 +8,10 @@
 #include "ccs_internal.h"
 #include "dispatch.cuh"
 #include "search_kernel.cuh"
-#include "search_phased.cuh"
 
 using namespace ccs;
 
 namespace ccs {
-
-constexpr int SEARCH_THREADS = 256;
 
 int ensure_search_buffers(ccs_handle* h, uint32_t slots) {
     CCS_CUDA_TRY(cudaSetDevice(h->device));
@@ -27,6 +24,7 @@ int ensure_search_buffers(ccs_handle* h, uint32_t slots) {
         }
     }
     if (!h->d_q) CCS_CUDA_TRY(cudaMalloc(&h->d_q, sizeof(QueueState)));
+    if (!h->d_don) CCS_CUDA_TRY(cudaMalloc(&h->d_don, sizeof(DonationCell) * DON_CELLS));
     if (slots > h->slot_cap) {
         cudaFree(h->d_slots);
         cudaFree(h->d_ring);
@@ -78,6 +76,13 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
     P->move_min = o && o->move_min > 0 ? (uint32_t)o->move_min : 8u;
     P->move_age = o && o->move_age > 0 ? (uint32_t)o->move_age : 4u;
     P->probe_min = o && o->probe_min > 0 ? (uint32_t)o->probe_min : 16u;
+    // Work stealing: cells of the handle, on unless opts->steal < 0.
+    const bool steal = h->d_don && !(o && o->steal < 0);
+    P->don = steal ? h->d_don : nullptr;
+    P->don_cap = steal ? DON_CELLS : 0u;
+    P->don_target = DON_CELLS / 4;
+    P->don_min_depth = o && o->steal_depth > 0 ? (uint32_t)o->steal_depth : 6u;
+    P->don_period = 64;  // a power of two
     P->done_log = nullptr;
     P->done_log_cap = 0;
 }
@@ -86,50 +91,30 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
 // 256 threads x 2 blocks per SM (registers for every value, no spills; the throughput kernel);
 // 2 = the same with sibling lookahead (two probe chains per lane: lower latency when few cubes
 // are searched, more probes); 3 = phase-ordered, 256 x 3 (80 registers); 4 = loop control,
-// frames in registers, 256 x 2; 5 = loop control, frames in shared memory, 512 x 2.
+// frames in registers, 256 x 2; 5 = loop control, frames in shared memory, 512 x 2;
+// 6 = phase-ordered, 128 x 4 (4 warps per block); 7 = phase-ordered, 512 x 1 (16 warps per block).
 // 0 = automatic: 2 for fewer than 64 cubes (and for the server), else 1.
 int resolve_variant(const ccs_solve_opts* o, int cubes) {
     int v = o ? o->variant : 0;
-    if (v <= 0 || v > 5) v = cubes < 64 ? 2 : 1;
+    if (v <= 0 || v > 7) v = cubes < 64 ? 2 : 1;
     return v;
 }
 
 int grid_for(ccs_handle* h, const ccs_solve_opts* o, int variant) {
-    int bps = o && o->blocks_per_sm > 0 ? o->blocks_per_sm : (variant == 3 ? 3 : 2);
+    int bps = o && o->blocks_per_sm > 0 ? o->blocks_per_sm
+                                         : (variant == 3 ? 3 : variant == 6 ? 4 : variant == 7 ? 1 : 2);
     return bps * h->sms;
 }
 
-template <int MODE, int NEC, int FMT, int THREADS, bool SMEM, int MINB>
-int launch_variant(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream) {
-    auto* k = search_kernel<MODE, NEC, FMT, THREADS, SMEM, MINB>;
-    constexpr size_t dyn = search_dyn_smem<SMEM, THREADS>();
-    if (dyn) CCS_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-    k<<<grid, THREADS, dyn, stream>>>(h->d_tables, P);
-    CCS_CUDA_TRY(cudaGetLastError());
-    return CCS_OK;
-}
+// The search kernels of each kind are compiled in their own translation unit (search_launch.cuh,
+// launch_*.cu), so the instantiations build in parallel.
+template <int MODE, int NEC>
+int launch_kind(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream, int variant);
 
-template <int MODE, int NEC, int FMT, int THREADS, int MINB, bool LOOKAHEAD = false>
-int launch_phased(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream) {
-    auto* k = search_kernel_phased<MODE, NEC, FMT, THREADS, MINB, LOOKAHEAD>;
-    constexpr size_t dyn = search_dyn_smem<true, THREADS>();
-    if (dyn) CCS_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-    k<<<grid, THREADS, dyn, stream>>>(h->d_tables, P);
-    CCS_CUDA_TRY(cudaGetLastError());
-    return CCS_OK;
-}
-
-// variant: a resolved one (1..5).
+// variant: a resolved one (1..7).
 int launch_kernel(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream, int variant) {
     return dispatch_kind(h->kind, [&](auto M, auto N) {
-        return dispatch_fmt(h->format, [&](auto F) {
-            constexpr int MODE = decltype(M)::value, NEC = decltype(N)::value, FMT = decltype(F)::value;
-            if (variant == 2) return launch_phased<MODE, NEC, FMT, 256, 2, true>(h, P, grid, stream);
-            if (variant == 3) return launch_phased<MODE, NEC, FMT, 256, 3>(h, P, grid, stream);
-            if (variant == 4) return launch_variant<MODE, NEC, FMT, SEARCH_THREADS, false, 2>(h, P, grid, stream);
-            if (variant == 5) return launch_variant<MODE, NEC, FMT, 512, true, 2>(h, P, grid, stream);
-            return launch_phased<MODE, NEC, FMT, 256, 2>(h, P, grid, stream);
-        });
+        return launch_kind<decltype(M)::value, decltype(N)::value>(h, P, grid, stream, variant);
     });
 }
 
@@ -193,6 +178,7 @@ extern "C" int ccs_solve_tables(ccs_handle* h, const uint32_t* states, const uin
     cudaStream_t st = h->stream;
     CCS_CUDA_TRY(cudaMemcpyAsync(h->d_slots, host.data(), sizeof(Slot) * n, cudaMemcpyHostToDevice, st));
     CCS_CUDA_TRY(cudaMemsetAsync(h->d_ring, 0xFF, sizeof(unsigned long long) * (h->ring_cap + h->slot_cap), st));
+    CCS_CUDA_TRY(cudaMemsetAsync(h->d_don, 0, sizeof(DonationCell) * DON_CELLS, st));
     CCS_CUDA_TRY(cudaMemcpyAsync(P.admit, admit.data(), 8ull * n, cudaMemcpyHostToDevice, st));
     CCS_CUDA_TRY(cudaMemcpyAsync(h->d_q, &q, sizeof q, cudaMemcpyHostToDevice, st));
 
@@ -226,11 +212,29 @@ extern "C" int ccs_solve_tables(ccs_handle* h, const uint32_t* states, const uin
     }
     h->last_kernel_ms = kernel_ms;
     h->last_probes = q.probes;
+    h->last_donated = q.donated;
     h->last_launches = launches;
+    // host <-> device bytes of this call: cube slots, admission entries and the queue state in;
+    // the queue state after every launch and the cube slots out
+    h->last_h2d = (sizeof(Slot) + 8ull) * (uint64_t)n + sizeof(QueueState);
+    h->last_d2h = sizeof(QueueState) * (uint64_t)launches + sizeof(Slot) * (uint64_t)n;
     CCS_CUDA_TRY(cudaMemcpyAsync(host.data(), h->d_slots, sizeof(Slot) * n, cudaMemcpyDeviceToHost, st));
     CCS_CUDA_TRY(cudaStreamSynchronize(st));
     for (int i = 0; i < n; ++i) fill_result(host[i], &results[i]);
     if (q.error & ERR_BOUND) return fail(CCS_E_CHECK, "a search passed the largest possible bound");
+    return CCS_OK;
+}
+
+extern "C" int ccs_last_solve_io_bytes(ccs_handle* h, uint64_t* h2d, uint64_t* d2h) {
+    if (!h) return fail(CCS_E_ARG, "NULL handle");
+    if (h2d) *h2d = h->last_h2d;
+    if (d2h) *d2h = h->last_d2h;
+    return CCS_OK;
+}
+
+extern "C" int ccs_last_solve_donations(ccs_handle* h, uint64_t* donated) {
+    if (!h || !donated) return fail(CCS_E_ARG, "NULL argument");
+    *donated = h->last_donated;
     return CCS_OK;
 }
 

@@ -49,6 +49,8 @@ class SolveOpts(ctypes.Structure):
         ("move_min", ctypes.c_int),
         ("move_age", ctypes.c_int),
         ("probe_min", ctypes.c_int),
+        ("steal", ctypes.c_int),
+        ("steal_depth", ctypes.c_int),
     ]
 
 
@@ -78,6 +80,8 @@ _SIGS = {
     "ccs_register_group_kind": [ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
     "ccs_kind_tables": [ctypes.c_char_p] + [ctypes.c_void_p] * 5,
     "ccs_set_kind": [ctypes.c_void_p, ctypes.c_char_p],
+    "ccs_last_solve_donations": [ctypes.c_void_p, _P(ctypes.c_uint64)],
+    "ccs_last_solve_io_bytes": [ctypes.c_void_p, _P(ctypes.c_uint64), _P(ctypes.c_uint64)],
     "ccs_load_table": [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p],
     "ccs_build_table": [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
                         ctypes.c_void_p, ctypes.c_int, _P(ctypes.c_int), _P(ctypes.c_double), LOG_FN],
@@ -168,9 +172,10 @@ def gather_bench(device: int = 0, nbytes: int = 8 << 30, rounds: int = 64) -> tu
 def solve_opts(base_plen: int = 4, deeper_at: tuple[float, float] = (5e7, 3e9), blocks_per_sm: int = 0,
                threads: int = 0, timeout_s: float = 0.0, spread: int = 0, variant: int = 0,
                shallow_at: tuple[float, float] = (0.0, 0.0), move_min: int = 0, move_age: int = 0,
-               probe_min: int = 0) -> SolveOpts:
+               probe_min: int = 0, steal: int = 0, steal_depth: int = 0) -> SolveOpts:
     return SolveOpts(base_plen, float(deeper_at[0]), float(deeper_at[1]), blocks_per_sm, threads, timeout_s, spread,
-                     variant, float(shallow_at[0]), float(shallow_at[1]), move_min, move_age, probe_min)
+                     variant, float(shallow_at[0]), float(shallow_at[1]), move_min, move_age, probe_min, steal,
+                     steal_depth)
 
 
 class Handle:
@@ -276,6 +281,20 @@ class Handle:
         ms, probes, launches = ctypes.c_double(), ctypes.c_uint64(), ctypes.c_int()
         check(lib.ccs_last_solve_stats(self._h, ctypes.byref(ms), ctypes.byref(probes), ctypes.byref(launches)))
         return ms.value, probes.value, launches.value
+
+    def last_solve_io_bytes(self) -> tuple[int, int]:
+        """(host -> device, device -> host) bytes the last solve copied."""
+
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        check(lib.ccs_last_solve_io_bytes(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def last_solve_donations(self) -> int:
+        """Subtrees the last solve's lanes donated to idle lanes (work stealing)."""
+
+        n = ctypes.c_uint64()
+        check(lib.ccs_last_solve_donations(self._h, ctypes.byref(n)))
+        return n.value
 
     # server
     def server_start(self, slots: int, opts: SolveOpts | None = None) -> None:

@@ -119,13 +119,17 @@ typedef struct ccs_solve_opts {
     double timeout_s;         /* give up after this long (0: no limit)                      */
     int spread;               /* lanes work on up to this many queued cubes at once (0: 4096) */
     int variant;              /* search kernel: 0 automatic, 1 throughput, 2 sibling lookahead */
-                              /*   (latency), 3-5 other launch shapes (see solve.cu)            */
+                              /*   (latency), 3-7 other launch shapes: 3 = 256 x 3 blocks/SM,  */
+                              /*   6 = 128 x 4, 7 = 512 x 1 (4-5: loop-control forms)           */
     double shallow_at0;       /* an iteration of < this many nodes makes the next one use a    */
     double shallow_at1;       /*   prefix one move shorter (0: 1e5 / 1.5e6, < 0: off)          */
     int move_min;             /* lanes waiting before a frame-update pass runs (0: 8)          */
     int move_age;             /* warp iterations a lane may wait for it (0: 4)                 */
     int probe_min;            /* a warp keeps probing (pruned children -> next sibling) while  */
                               /*   at least this many lanes have a probe (0: default, > 32: off) */
+    int steal;                /* work stealing: lanes donate unexplored subtrees to idle lanes  */
+                              /*   (variants 1, 3, 6, 7; 0: on, < 0: off)                       */
+    int steal_depth;          /* a donated subtree has at least this many moves to the bound (0: 6) */
 } ccs_solve_opts;
 
 typedef struct ccs_result {
@@ -163,6 +167,14 @@ int ccs_solve_noalloc(ccs_handle* h, const uint32_t* states, int n, const ccs_so
 
 /* Device time of the last ccs_solve's search kernels (ms) and its total table probes. */
 int ccs_last_solve_stats(ccs_handle* h, double* kernel_ms, uint64_t* probes, int* launches);
+
+/* Bytes the last ccs_solve copied host -> device (cube slots, admission entries, queue state) and
+ * device -> host (queue state after each launch, cube slots). */
+int ccs_last_solve_io_bytes(ccs_handle* h, uint64_t* h2d, uint64_t* d2h);
+
+/* Subtrees the last ccs_solve's lanes donated to idle lanes (work stealing; no counterpart in the
+ * reference, whose work items are fixed per bound, solver.py:189-195). */
+int ccs_last_solve_donations(ccs_handle* h, uint64_t* donated);
 
 /* Random 32-byte sector gather ceiling of a device (the table probes' memory roofline): random
  * sector loads from a `bytes` buffer, 8 in flight per thread; sectors_per_s and the time. */

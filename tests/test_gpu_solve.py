@@ -94,3 +94,49 @@ def test_illegal_state_is_rejected():
     bad = state_words([CubieState(ep=(1, 0) + tuple(range(2, 12)))])
     with pytest.raises(native.CcsError, match="not a legal position"):
         h.solve(bad)
+
+
+def test_work_stealing_keeps_lengths_and_iteration_nodes(lengths_golden):
+    """Donated subtrees are searched exactly once: with stealing on (and forced often by a small
+    minimum depth) every completed iteration has the same node count as without it, the lengths
+    equal the reference's, and subtrees were in fact donated."""
+
+    h = resident_handle("d4")
+    # fewer than 32 cubes and no deeper prefixes: prefix lengths then do not depend on timing
+    cubes = lengths_golden["distance20"][:4] + [lengths_golden["hard19"]] + lengths_golden["random1000"][:26]
+    states = [_state(parse_moves(c["scramble"])) for c in cubes]
+    words = state_words(states)
+    base = dict(timeout_s=900, variant=1, deeper_at=(1e18, 1e18))
+    off = h.solve(words, native.solve_opts(steal=-1, **base))
+    assert h.last_solve_donations() == 0
+    for depth in (6, 3):
+        on = h.solve(words, native.solve_opts(steal=0, steal_depth=depth, **base))
+        assert h.last_solve_donations() > 0
+        _check_solutions(states, on)
+        assert [r.length for r in on] == [r.length for r in off] == [c["length"] for c in cubes]
+        for a, b in zip(on, off):  # every iteration before the last one was searched in full
+            assert list(a.iter_nodes[: a.length]) == list(b.iter_nodes[: b.length])
+
+
+def test_launch_shapes_agree(lengths_golden):
+    """The 128 x 4 and 512 x 1 launch shapes (and the others) give the reference's lengths."""
+
+    h = resident_handle("d4t")
+    cubes = lengths_golden["random1000"][300:364]
+    words = state_words([_state(parse_moves(c["scramble"])) for c in cubes])
+    for variant in (1, 2, 3, 4, 5, 6, 7):
+        res = h.solve(words, native.solve_opts(timeout_s=600, variant=variant))
+        assert [r.length for r in res] == [c["length"] for c in cubes], variant
+    h2d, d2h = h.last_solve_io_bytes()
+    assert h2d > 64 * 416 and d2h > 64 * 416
+
+
+def test_lone_superflip_with_stealing(lengths_golden):
+    """A lone hard cube spreads over the GPU through donated subtrees: the superflip on d4t."""
+
+    h = resident_handle("d4t")
+    c = lengths_golden["superflip"]
+    words = state_words([_state(parse_moves(c["scramble"]))])
+    res = h.solve(words, native.solve_opts(timeout_s=900, variant=1))
+    assert res[0].length == c["length"]
+    assert h.last_solve_donations() > 0
