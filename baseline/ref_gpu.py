@@ -200,7 +200,7 @@ class RefTables:
 
 
 def canonical_prefixes(length: int) -> np.ndarray:
-    from cuda_cube_solver.solver import canonical_prefixes as cp
+    from cuda_cube_solver.prefixes import canonical_prefixes as cp
 
     return np.ascontiguousarray(cp(length))
 
@@ -234,7 +234,7 @@ class RefSolver:
 
     def root_h(self, states) -> tuple[np.ndarray, np.ndarray]:
         from cuda_cube_solver.device import state_words
-        from cuda_cube_solver.solver import frames
+        from cuda_cube_solver.prefixes import frames
 
         words = state_words([f for s in states for f in frames(s)])
         n = len(words)

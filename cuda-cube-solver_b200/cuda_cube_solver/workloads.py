@@ -6,11 +6,18 @@
   a random corner and edge permutation (edges 10 and 11 swapped when the parities differ), seven
   random twists and eleven random flips, the last orientation of each closing its sum.
 * ``superflip``: every edge flipped in place.
+* ``batched_mix``: the batched configuration -- 4,096 uniform cubes of seed 2 in which 5% (205)
+  are replaced by hard positions: uniform cubes of the seed-20 stream whose optimal length is at
+  least 19 (their stream positions are listed in ``data/hard20.json``, written by
+  ``data/make_hard20.py`` from GPU solves and checked against the reference's kernels) and the
+  superflip, at positions drawn by ``np.random.default_rng(4)``.
 """
 
 from __future__ import annotations
 
+import json
 import random
+from pathlib import Path
 
 import numpy as np
 
@@ -53,3 +60,32 @@ def uniform_cubes(n: int, seed: int = 1) -> list[CubieState]:
 
 def superflip() -> CubieState:
     return CubieState(eo=(1,) * 12)
+
+
+HARD20 = Path(__file__).with_name("data") / "hard20.json"
+
+
+def hard20() -> dict:
+    """The seed-20 stream's cubes of optimal length >= 19: stream indices and lengths."""
+
+    return json.loads(HARD20.read_text())
+
+
+def batched_mix(n: int = 4096, seed: int = 2, hard_frac: float = 0.05) -> tuple[list[CubieState], dict[int, int]]:
+    """``n`` uniform cubes of ``seed`` with ``round(hard_frac * n)`` of them replaced by hard
+    positions (the first ones of ``hard20()`` and, last, the superflip).  Returns the cubes and
+    {position: known optimal length} of the hard ones."""
+
+    cubes = uniform_cubes(n, seed=seed)
+    n_hard = max(1, int(round(hard_frac * n)))
+    info = hard20()
+    if n_hard - 1 > len(info["indices"]):
+        raise ValueError(f"{n_hard - 1} hard cubes asked for; data/hard20.json lists {len(info['indices'])}")
+    stream = uniform_cubes(info["indices"][n_hard - 2] + 1, seed=20) if n_hard > 1 else []
+    hard = [(stream[i], L) for i, L in zip(info["indices"][: n_hard - 1], info["lengths"])] + [(superflip(), 20)]
+    where = np.random.default_rng(4).choice(n, size=len(hard), replace=False)
+    known = {}
+    for pos, (cube, length) in zip(where, hard):
+        cubes[int(pos)] = cube
+        known[int(pos)] = length
+    return cubes, known
