@@ -3,17 +3,19 @@ GPU, table and batch size by measuring them.
 
 Knobs (``native.SolveOpts``):
 
-* ``variant``: search kernel -- 1 = throughput (256 threads x 2 blocks per SM), 2 = sibling
-  lookahead (two probe chains per lane: lower latency for few cubes), 3 = 256 x 3 blocks per SM;
-  0 = the library's automatic choice;
-* ``base_plen``: cut depth of the work items (prefix length of a cube's iterations);
-* ``move_min`` / ``move_age``: how many lanes wait, and for how many iterations, before the
-  frame-update pass (push / pop) runs -- the depth of the lanes' update pipeline;
-* ``spread``: over how many queued cubes the lanes spread.
+* ``variant``: search kernel and launch shape -- 1 = 256 threads x 2 blocks per SM (the
+  throughput kernel), 2 = the same with sibling lookahead (two probe chains per lane), 3 = 256 x
+  3, 6 = 128 x 4 (4 warps per block), 7 = 512 x 1 (16 warps per block);
+* ``base_plen``: cut depth of the work items (prefix length of a cube's iterations), 3-6;
+* ``move`` = (``move_min``, ``move_age``): how many lanes wait, and for how many iterations,
+  before the frame-update pass (push / pop) runs -- the depth of the lanes' update pipeline, 1-16;
+* ``steal_depth``: the smallest subtree (moves left to the bound) a lane donates to idle lanes;
+* ``spread``: over how many queued cubes the lanes spread;
+* ``probe_min``: a warp keeps probing while at least this many lanes have a probe.
 
 Coordinate descent from the library defaults: each knob in turn takes the value with the best
-device time on the sample (the same cubes every time), twice round.  Results are cached in a JSON
-file keyed by GPU name, table and batch-size bucket, and ``GpuSolver`` picks them up.
+device time on the sample (the same cubes every time), within a time budget.  Results are cached
+in a JSON file keyed by GPU name, table and batch-size bucket, and ``GpuSolver`` picks them up.
 """
 
 from __future__ import annotations
@@ -29,19 +31,20 @@ from cuda_cube_solver.device import state_words
 CACHE = Path(os.environ.get("CCS_TUNE_CACHE", Path.home() / ".cache" / "cuda_cube_solver" / "autotune.json"))
 
 SPACE = {
-    "variant": [1, 2, 3],
-    "base_plen": [3, 4, 5],
-    "move": [(4, 2), (8, 4), (12, 6), (16, 8)],
+    "variant": [1, 2, 3, 6, 7],
+    "base_plen": [3, 4, 5, 6],
+    "move": [(1, 1), (4, 2), (8, 4), (16, 8)],
+    "steal_depth": [4, 6, 8],
     "spread": [512, 1024, 4096],
     "probe_min": [12, 16, 20, 24],
 }
-DEFAULT = {"variant": 0, "base_plen": 4, "move": (8, 4), "spread": 4096, "probe_min": 16}
+DEFAULT = {"variant": 1, "base_plen": 4, "move": (8, 4), "steal_depth": 6, "spread": 4096, "probe_min": 16}
 
 
 def opts_of(cfg: dict, timeout_s: float = 600.0) -> native.SolveOpts:
     return native.solve_opts(base_plen=cfg["base_plen"], variant=cfg["variant"], spread=cfg["spread"],
                              move_min=cfg["move"][0], move_age=cfg["move"][1], timeout_s=timeout_s,
-                             probe_min=cfg.get("probe_min", 0))
+                             probe_min=cfg.get("probe_min", 0), steal_depth=cfg.get("steal_depth", 0))
 
 
 def batch_bucket(n: int) -> str:
@@ -59,19 +62,25 @@ def measure(handle: native.Handle, words, cfg: dict) -> float:
     return handle.last_solve_stats()[0] / 1000.0
 
 
-def tune(handle: native.Handle, states, table: str, rounds: int = 2, log=None) -> dict:
-    """Best settings for ``states`` (a representative sample) on the handle's table."""
+def tune(handle: native.Handle, states, table: str, rounds: int = 2, log=None, budget_s: float = 0.0) -> dict:
+    """Best settings for ``states`` (a representative sample) on the handle's table; with
+    ``budget_s`` > 0 the descent stops once that much time has passed (the best so far stands)."""
 
     words = state_words(states)
+    t_start = time.perf_counter()
     best = dict(DEFAULT)
     measure(handle, words, best)  # warm-up
     best_t = measure(handle, words, best)
     trials = [(dict(best), best_t)]
+    out_of_time = False
     for _ in range(rounds):
         for knob, values in SPACE.items():
             for v in values:
                 if v == best[knob]:
                     continue
+                if budget_s > 0 and time.perf_counter() - t_start > budget_s:
+                    out_of_time = True
+                    break
                 cfg = dict(best, **{knob: v})
                 t = measure(handle, words, cfg)
                 trials.append((cfg, t))
@@ -80,7 +89,9 @@ def tune(handle: native.Handle, states, table: str, rounds: int = 2, log=None) -
                 if t < best_t:
                     best, best_t = cfg, t
     return {"config": best, "cubes_per_s": len(states) / best_t, "trials": len(trials),
-            "default_cubes_per_s": len(states) / trials[0][1], "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
+            "default_cubes_per_s": len(states) / trials[0][1], "complete": not out_of_time,
+            "seconds": time.perf_counter() - t_start, "sample": f"{len(states)} cubes",
+            "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
 
 
 def gpu_name(device: int = 0) -> str:

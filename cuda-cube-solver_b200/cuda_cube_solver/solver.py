@@ -178,18 +178,20 @@ class GpuSolver:
             o.variant, o.base_plen, o.spread = tuned["variant"], tuned["base_plen"], tuned["spread"]
             o.move_min, o.move_age = tuned["move"]
             o.probe_min = tuned.get("probe_min", 0)
+            o.steal_depth = tuned.get("steal_depth", 0)
         return o
 
     @property
     def table_name(self) -> str:
         return self.kind.name if self.table_format == "block" else f"{self.kind.name}-b3"
 
-    def autotune(self, sample: list[CubieState], log=None, save: bool = True) -> dict:
-        """Measure the kernel settings on ``sample`` and use the best from now on."""
+    def autotune(self, sample: list[CubieState], log=None, save: bool = True, budget_s: float = 0.0) -> dict:
+        """Measure the kernel settings on ``sample`` and use the best from now on (within
+        ``budget_s`` seconds when it is > 0)."""
 
         from cuda_cube_solver import autotune
 
-        result = autotune.tune(self.handle, sample, self.table_name, log=log)
+        result = autotune.tune(self.handle, sample, self.table_name, log=log, budget_s=budget_s)
         self.tuned = result["config"]
         if save:
             autotune.save(result, self.table_name, len(sample), self.handle.device)

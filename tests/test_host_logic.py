@@ -13,7 +13,7 @@ from cuda_cube_solver import autotune, serving, workloads
 class FakeHandle:
     """Device time of a solve as a function of the settings, smallest at BEST."""
 
-    BEST = {"variant": 2, "base_plen": 4, "move": (4, 2), "spread": 1024, "probe_min": 12}
+    BEST = {"variant": 2, "base_plen": 5, "move": (4, 2), "steal_depth": 4, "spread": 1024, "probe_min": 12}
 
     def __init__(self):
         self.calls = []
@@ -22,7 +22,7 @@ class FakeHandle:
     def solve(self, words, opts):
         self.calls.append(opts)
         cfg = {"variant": opts.variant, "base_plen": opts.base_plen, "move": (opts.move_min, opts.move_age),
-               "spread": opts.spread, "probe_min": opts.probe_min}
+               "steal_depth": opts.steal_depth, "spread": opts.spread, "probe_min": opts.probe_min}
         self._ms = 100.0 + sum(0.0 if cfg[k] == v else 7.0 + abs(hash((k, cfg[k]))) % 5 for k, v in self.BEST.items())
         return []
 
@@ -38,6 +38,17 @@ def test_autotune_finds_the_best_settings():
     assert result["cubes_per_s"] == len(sample) / 0.1
     assert result["trials"] == len(h.calls) - 1  # the first call is the warm-up
     assert result["cubes_per_s"] >= result["default_cubes_per_s"]
+    assert result["complete"]
+
+
+def test_autotune_stops_at_its_budget():
+    h = FakeHandle()
+    result = autotune.tune(h, workloads.uniform_cubes(4, seed=9), "d4t", rounds=2, budget_s=1e-9)
+    assert not result["complete"] and result["trials"] == 1 and len(h.calls) == 2
+    # the space covers cut depth 3-6, 4-16 warps per block (variants 6, 1, 7) and update depth 1-16
+    assert autotune.SPACE["base_plen"] == [3, 4, 5, 6]
+    assert {6, 1, 7} <= set(autotune.SPACE["variant"])
+    assert [m for m, _ in autotune.SPACE["move"]] == [1, 4, 8, 16]
 
 
 def test_autotune_cache_round_trip(tmp_path, monkeypatch):
