@@ -3,4 +3,5 @@
 
 namespace ccs {
 template int launch_kind<KIND_GEN, 8>(ccs_handle*, const SearchParams&, int, cudaStream_t, int);
+template int kernel_footprint_kind<KIND_GEN, 8>(ccs_handle*, int, size_t*, int*);
 }  // namespace ccs

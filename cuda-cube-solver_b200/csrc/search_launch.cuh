@@ -44,4 +44,26 @@ int launch_kind(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t str
     });
 }
 
+// Local memory (per-lane DFS stacks) and threads per block of a variant's kernel.
+template <int MODE, int NEC>
+int kernel_footprint_kind(ccs_handle* h, int variant, size_t* local_bytes, int* threads) {
+    return dispatch_fmt(h->format, [&](auto F) {
+        constexpr int FMT = decltype(F)::value;
+        cudaFuncAttributes a{};
+        int t = 256;
+        cudaError_t e;
+        if (variant == 2) e = cudaFuncGetAttributes(&a, search_kernel_phased<MODE, NEC, FMT, 256, 2, true>);
+        else if (variant == 3) e = cudaFuncGetAttributes(&a, search_kernel_phased<MODE, NEC, FMT, 256, 3>);
+        else if (variant == 4) e = cudaFuncGetAttributes(&a, search_kernel<MODE, NEC, FMT, 256, false, 2>);
+        else if (variant == 5) e = (t = 512, cudaFuncGetAttributes(&a, search_kernel<MODE, NEC, FMT, 512, true, 2>));
+        else if (variant == 6) e = (t = 128, cudaFuncGetAttributes(&a, search_kernel_phased<MODE, NEC, FMT, 128, 4>));
+        else if (variant == 7) e = (t = 512, cudaFuncGetAttributes(&a, search_kernel_phased<MODE, NEC, FMT, 512, 1>));
+        else e = cudaFuncGetAttributes(&a, search_kernel_phased<MODE, NEC, FMT, 256, 2>);
+        CCS_CUDA_TRY(e);
+        *local_bytes = a.localSizeBytes;
+        *threads = t;
+        return CCS_OK;
+    });
+}
+
 }  // namespace ccs

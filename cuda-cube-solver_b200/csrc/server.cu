@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "ccs_internal.h"
+#include "dispatch.cuh"
 #include "search_kernel.cuh"
 
 using namespace ccs;
@@ -48,6 +49,10 @@ struct Server {
     std::vector<uint64_t> slot_request;
     std::vector<uint32_t> slot_gen;  // reuse count of each slot
     uint32_t in_flight = 0;
+    // Device-memory budget (0: none): a cube is admitted only while the fixed footprint plus the
+    // bytes of every cube in flight stays within it.
+    uint64_t budget = 0, fixed_bytes = 0, per_cube = 0;
+    uint32_t peak_in_flight = 0;
 
     std::mutex mu;
     std::condition_variable cv;
@@ -86,7 +91,8 @@ int Server::step() {
     std::vector<std::pair<uint64_t, std::array<uint32_t, 6>>> take;
     {
         std::lock_guard<std::mutex> lock(mu);
-        while (!pending.empty() && take.size() < free_slots.size()) {
+        while (!pending.empty() && take.size() < free_slots.size() &&
+               (budget == 0 || fixed_bytes + (in_flight + take.size() + 1) * per_cube <= budget)) {
             take.push_back(pending.front());
             pending.pop_front();
         }
@@ -106,6 +112,7 @@ int Server::step() {
             CCS_CUDA_TRY(cudaStreamSynchronize(copy));  // slot and entry land before the tail moves
             ++in_flight;
         }
+        if (in_flight > peak_in_flight) peak_in_flight = in_flight;
         unsigned long long tail = admit_pos;
         CCS_CUDA_TRY(cudaMemcpyAsync(&h->d_q->admit_tail, &tail, 8, cudaMemcpyHostToDevice, copy));
         CCS_CUDA_TRY(cudaStreamSynchronize(copy));
@@ -162,7 +169,67 @@ int server_stop(ccs_handle* h) {
     return CCS_OK;
 }
 
+// Bytes of device memory a cube in flight holds: its slot, four work-ring positions and its
+// admission entry.  The search stacks are per lane (local memory of the persistent launch), fixed
+// by the grid whatever the number of cubes, so they count in the fixed footprint.
+constexpr uint64_t SERVER_BYTES_PER_CUBE = sizeof(Slot) + 5ull * sizeof(unsigned long long);
+constexpr uint32_t SERVER_MAX_SLOTS = 65536;
+
+template <int MODE, int NEC>
+int kernel_footprint_kind(ccs_handle* h, int variant, size_t* local_bytes, int* threads);
+
+// Device memory the server holds whatever the number of cubes: resident tables, constants,
+// prefix lists, queue state, donation cells and the persistent launch's per-lane stacks.
+int server_fixed_bytes(ccs_handle* h, const ccs_solve_opts* opts, uint64_t* out) {
+    const int variant = resolve_variant(opts, 0);
+    const int grid = grid_for(h, opts, variant);
+    size_t local = 0;
+    int threads = 0;
+    CCS_TRY(dispatch_kind(h->kind, [&](auto M, auto N) {
+        return kernel_footprint_kind<decltype(M)::value, decltype(N)::value>(h, variant, &local, &threads);
+    }));
+    uint64_t prefixes = 0;
+    for (int L = 0; L <= MAX_PLEN; ++L) prefixes += 4ull * h->n_prefix[L];
+    *out = h->table_bytes + h->table2_bytes + sizeof(DevTables) + 153090ull * 4 + 9930ull * 6 + prefixes +
+           sizeof(QueueState) + sizeof(DonationCell) * DON_CELLS + (uint64_t)local * threads * grid;
+    return CCS_OK;
+}
+
 }  // namespace ccs
+
+extern "C" int ccs_server_start_budget(ccs_handle* h, uint64_t budget_bytes, const ccs_solve_opts* opts,
+                                       int* slots_out) {
+    if (!h) return fail(CCS_E_ARG, "NULL handle");
+    if (!h->d_table) return fail(CCS_E_STATE, "no table loaded");
+    CCS_TRY(ensure_search_buffers(h, 1));  // (the prefix lists count in the fixed footprint)
+    uint64_t fixed = 0;
+    CCS_TRY(server_fixed_bytes(h, opts, &fixed));
+    if (budget_bytes < fixed + SERVER_BYTES_PER_CUBE)
+        return fail(CCS_E_NOMEM, "budget of %llu bytes: the tables, constants and stacks alone take %llu",
+                    (unsigned long long)budget_bytes, (unsigned long long)fixed);
+    const uint64_t fit = (budget_bytes - fixed) / SERVER_BYTES_PER_CUBE;
+    const int slots = (int)(fit < SERVER_MAX_SLOTS ? fit : SERVER_MAX_SLOTS);
+    CCS_TRY(ccs_server_start(h, slots, opts));
+    Server* s = h->server;
+    s->budget = budget_bytes;
+    s->fixed_bytes = fixed;
+    s->per_cube = SERVER_BYTES_PER_CUBE;
+    if (slots_out) *slots_out = slots;
+    return CCS_OK;
+}
+
+extern "C" int ccs_server_memory(ccs_handle* h, uint64_t* budget, uint64_t* fixed, uint64_t* per_cube,
+                                 uint64_t* peak_in_flight) {
+    if (!h) return fail(CCS_E_ARG, "NULL handle");
+    Server* s = h->server;
+    if (!s) return fail(CCS_E_STATE, "server not running");
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (budget) *budget = s->budget;
+    if (fixed) *fixed = s->fixed_bytes;
+    if (per_cube) *per_cube = SERVER_BYTES_PER_CUBE;
+    if (peak_in_flight) *peak_in_flight = s->peak_in_flight;
+    return CCS_OK;
+}
 
 extern "C" int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* opts) {
     if (!h || slots <= 0) return fail(CCS_E_ARG, "bad arguments");

@@ -81,6 +81,8 @@ _SIGS = {
     "ccs_kind_tables": [ctypes.c_char_p] + [ctypes.c_void_p] * 5,
     "ccs_set_kind": [ctypes.c_void_p, ctypes.c_char_p],
     "ccs_last_solve_donations": [ctypes.c_void_p, _P(ctypes.c_uint64)],
+    "ccs_server_start_budget": [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, _P(ctypes.c_int)],
+    "ccs_server_memory": [ctypes.c_void_p] + [_P(ctypes.c_uint64)] * 4,
     "ccs_last_solve_io_bytes": [ctypes.c_void_p, _P(ctypes.c_uint64), _P(ctypes.c_uint64)],
     "ccs_load_table": [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p],
     "ccs_build_table": [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
@@ -299,6 +301,19 @@ class Handle:
     # server
     def server_start(self, slots: int, opts: SolveOpts | None = None) -> None:
         check(lib.ccs_server_start(self._h, slots, ctypes.byref(opts or solve_opts())))
+
+    def server_start_budget(self, budget_bytes: int, opts: SolveOpts | None = None) -> int:
+        """Start the server with admission by device memory; returns the cubes the budget admits."""
+
+        slots = ctypes.c_int()
+        check(lib.ccs_server_start_budget(self._h, int(budget_bytes), ctypes.byref(opts or solve_opts()),
+                                          ctypes.byref(slots)))
+        return slots.value
+
+    def server_memory(self) -> dict:
+        v = [ctypes.c_uint64() for _ in range(4)]
+        check(lib.ccs_server_memory(self._h, *[ctypes.byref(x) for x in v]))
+        return dict(zip(("budget_bytes", "fixed_bytes", "bytes_per_cube", "peak_in_flight"), [x.value for x in v]))
 
     def server_submit(self, state: np.ndarray, table_id: int = 0) -> int:
         state = np.ascontiguousarray(state, dtype=np.uint32).reshape(5)

@@ -31,14 +31,25 @@ class Served:
 
 class Server:
     """Continuous batching on one handle (its table must be loaded).  ``flip_rule``: with a second
-    table attached, requests with at least this many flipped edges are searched with it."""
+    table attached, requests with at least this many flipped edges are searched with it.
+    ``budget_bytes``: admit cubes by device memory within this budget (tables and the other fixed
+    buffers included) instead of by a slot count."""
 
     def __init__(self, handle: native.Handle, slots: int = 1024, opts: native.SolveOpts | None = None,
-                 flip_rule: int | None = None):
+                 flip_rule: int | None = None, budget_bytes: int | None = None):
         self.h = handle
         self.flip_rule = flip_rule
-        self.h.server_start(slots, opts or native.solve_opts())
+        if budget_bytes:
+            self.slots = self.h.server_start_budget(budget_bytes, opts or native.solve_opts())
+        else:
+            self.h.server_start(slots, opts or native.solve_opts())
+            self.slots = slots
         self.submitted: dict[int, float] = {}
+
+    def memory(self) -> dict:
+        """Budget, fixed footprint, bytes per cube in flight and the peak number in flight."""
+
+        return dict(self.h.server_memory(), slots=self.slots)
 
     def submit(self, state: CubieState) -> int:
         words = state_words([state])

@@ -191,6 +191,19 @@ int ccs_probe_bench(ccs_handle* h, int n_states, int rounds, double* probes_per_
  * the GPU are admitted into free slots without waiting for the running ones.  slots <
  * 1,048,575; each takes 456 bytes of device memory (cube slot and ring positions). */
 int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* opts);
+
+/* ccs_server_start with admission by device memory (the serving loop of north_star; the reference
+ * has fixed --batch chunks only, __main__.py:129-133): the server holds a fixed footprint --
+ * resident tables, constants, prefix lists, queue state, work-stealing cells and the persistent
+ * launch's per-lane search stacks -- plus 456 bytes per cube in flight (its slot, ring positions
+ * and admission entry); a cube is admitted only while the total stays within budget_bytes.
+ * CCS_E_NOMEM if the fixed footprint alone exceeds the budget.  slots_out (may be NULL): the cubes
+ * the budget admits at once (at most 65,536). */
+int ccs_server_start_budget(ccs_handle* h, uint64_t budget_bytes, const ccs_solve_opts* opts, int* slots_out);
+
+/* The running server's budget (0: none), fixed footprint and bytes per cube in flight (bytes), and
+ * the most cubes it has held in flight at once. */
+int ccs_server_memory(ccs_handle* h, uint64_t* budget, uint64_t* fixed, uint64_t* per_cube, uint64_t* peak_in_flight);
 int ccs_server_submit(ccs_handle* h, const uint32_t* state, uint64_t* request_id);
 int ccs_server_submit_table(ccs_handle* h, const uint32_t* state, int table_id, uint64_t* request_id);
 int ccs_server_poll(ccs_handle* h, int max_out, uint64_t* request_ids, ccs_result* results, int* n_out);
