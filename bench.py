@@ -1,20 +1,34 @@
-"""Benchmark: optimal solves/s of uniformly random cubes on the d4t table, batched, on B200.
+"""Benchmark: optimal solves/s of the batched configuration on B200 (d4t table), beside plain
+one-at-a-time solving, the served stream and the reference's own builds.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference|reference-gpu]
 
-One step = one batched solve (libccs persistent launch) of B uniformly random cubes (seeded)
-against the d4t table resident in HBM.  The table is built on the GPU first (untimed, its build
-time is reported).  ``value`` = cubes / device time of the search launches (CUDA events on the
-library's stream), max over ranks; ``e2e`` = the same through the public API
-(``GpuSolver.solve`` with host CubieState lists: packing, host->device copy, search,
-device->host copy of the results, host verification of every solution).  ``plain`` = one cube
-per call (the drop-in path), with p50 / p99 per-cube latency.  Under torchrun each rank is an
-independent replica on its own GPU with its own cubes (weak scaling, no collective on the data
-path; NCCL only for the barrier and the max-over-ranks timing).
+One step = one batched solve through the public API (``GpuSolver.solve``: host cubes in,
+verified ``Solution`` objects out) of the batched workload: 4,096 uniform random cubes (seed 2)
+in which 5% (205) are replaced by hard positions -- 204 uniform cubes of the seed-20 stream whose
+optimal length is >= 19 and the superflip (``workloads.batched_mix``) -- on the d4t block table
+resident in HBM (7.8 GB, far larger than L2: every probe is a random 32-byte sector).
+
+* ``value``: cubes / device time of the search launches (CUDA events on the library's stream),
+  max over ranks.  ``e2e``: cubes / host wall time of the same ``GpuSolver.solve`` calls, which
+  include packing the states, the host->device copies, the search, the device->host copy of the
+  results and the host check of every solution.
+* The kernel settings come from the autotuner, run untimed on a separate sample first.
+* After the timed steps (untimed unless stated): the same batch on d4 (lengths must equal d4t's)
+  and with the flip-count rule; 1,024 uniform cubes alone; ``plain`` = 1,000 uniform cubes of
+  seed 1 solved one per call (p50 / p99 / worst); the reference's own kernels.cu with its
+  per-bound host loop on the same plain cubes (``reference_gpu``; lengths compared); the served
+  stream at 10 / 50 / 100 / 200 requests/s within a device-memory budget; the random-sector
+  gather ceiling; the CPU baseline.
+
+Under torchrun each rank is an independent replica on its own GPU with its own cubes (weak
+scaling; NCCL only for the barrier and the max-over-ranks timing).
 
 ``--impl reference``: the reference's method on the host's CPU cores -- the CPU oracle's IDA*
-(oracle/ccs_oracle.c, a restatement of the reference's search) over the same cubes and table,
-rank 0 only, bounded to a short sample.
+(oracle/ccs_oracle.c, a restatement of the reference's search) over the same cubes, on a table
+built by the reference's own BFS kernels (baseline/ref_gpu.py), all host threads, cubes finished
+in a fixed window; rank 0 only.  This arm never loads libccs.
+``--impl reference-gpu``: the reference's kernels.cu with its host loop on the plain cubes.
 """
 
 from __future__ import annotations
@@ -112,7 +126,7 @@ def dist_setup():
         backend = "nccl" if torch.cuda.is_available() else "gloo"
         if backend == "nccl":
             torch.cuda.set_device(local)
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=900))
     return world, rank, local
 
 
@@ -135,36 +149,53 @@ def max_over_ranks(x: float, world: int, local: int) -> float:
     return float(t.item())
 
 
-def shard(n_total: int, world: int, rank: int) -> slice:
-    """Replicas: rank r takes cubes [r * n, (r + 1) * n) of the seeded stream."""
+def rank_seed(seed: int, rank: int) -> int:
+    """Replicas: rank 0 solves the configuration's own cubes, rank r > 0 those of seed + 97 r."""
 
-    return slice(rank * n_total, (rank + 1) * n_total)
+    return seed + 97 * rank
 
 
-def cpu_arm(args, states, frames_words, table: np.ndarray, probes_per_cube: float | None) -> dict:
-    """The reference's method on host cores: the CPU oracle's IDA* over the cubes, all threads,
-    bounded by ``args.cpu_budget`` seconds.  Throughput counts finished cubes plus the unfinished
-    ones' work in cube units (their probes / mean probes of a cube)."""
+def config_table(args) -> str:
+    return args.kind if args.format == "block" else f"{args.kind}-b3"
+
+
+def workload_config(args, world: int) -> dict:
+    n_hard = int(round(0.05 * args.batch))
+    return {"workload": f"batched: {args.batch} uniform random cubes (seed {args.seed}) with {n_hard} (5%) replaced by "
+                        f"hard positions ({n_hard - 1} seed-20 uniform cubes of optimal length >= 19 and the superflip), "
+                        f"{config_table(args)} table resident in HBM, one batch per step per GPU",
+            "table": config_table(args), "batch": args.batch, "hard": n_hard, "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (7.8 GB table, random probes)"}
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU side: the oracle's IDA* (the reference's method restated) and the reference's cpu_gather
+
+
+def cpu_window(kind: str, fmt: str, table: np.ndarray, cubes, seconds: float, threads: int | None = None) -> dict:
+    """The oracle's IDA* on host threads over ``cubes`` (in order, each thread taking the next
+    cube) for a fixed window; throughput counts the cubes finished in the window only (the work on
+    cubes still open when it closes is dropped, which understates the CPU a little)."""
 
     sys.path.insert(0, str(ROOT / "oracle"))
     from oracle import Oracle
 
+    from cuda_cube_solver.device import state_words
+    from cuda_cube_solver.prefixes import frames
+
     o = Oracle()
-    o.set_kind(args.kind)
-    threads = os.cpu_count() or 1
-    n = min(len(frames_words), max(threads * 2, 8))
+    o.set_kind(kind)
+    threads = threads or os.cpu_count() or 1
+    fr = np.stack([state_words(frames(s)).reshape(30) for s in cubes])
     t0 = time.perf_counter()
-    lengths, _, _, probes = o.solve_many(table, args.format, frames_words[:n], threads=threads,
-                                        budget_s=args.cpu_budget)
+    lengths, _, _, probes = o.solve_many(table, fmt, fr, threads=threads, budget_s=seconds)
     dt = time.perf_counter() - t0
     done = lengths >= 0
-    per_cube = probes_per_cube or (float(probes[done].mean()) if done.any() else None)
-    units = float(done.sum()) + (float(probes[~done].sum()) / per_cube if per_cube else 0.0)
-    return {"value": units / dt, "unit": "cubes/s", "cores": threads, "kind": "port",
-            "sample": f"first {n} cubes of the workload, CPU oracle IDA* (oracle/ccs_oracle.c) on {threads} threads for "
-                      f"{dt:.1f} s: {int(done.sum())} solved, unfinished work counted at "
-                      f"{per_cube / 1e6 if per_cube else 0:.1f} M probes per cube",
-            "probes_per_s": float(probes.sum()) / dt, "probes_per_cube": per_cube}
+    return {"value": float(done.sum()) / dt, "unit": "cubes/s", "cores": threads, "kind": "port",
+            "sample": f"the workload's cubes in order, CPU oracle IDA* (oracle/ccs_oracle.c) on {threads} threads for "
+                      f"{dt:.1f} s: {int(done.sum())} cubes finished and counted, the cubes still open when the window "
+                      f"closed not counted",
+            "finished": int(done.sum()), "window_s": dt, "probes_per_s": float(probes.sum()) / dt}
 
 
 def reference_cpu_gather(probes_per_cube: float | None) -> dict | None:
@@ -191,282 +222,200 @@ def reference_cpu_gather(probes_per_cube: float | None) -> dict | None:
     return out
 
 
-def served_stream(args, solver, opts) -> dict:
-    """Config 5: Poisson arrivals (seed 3) into the continuous-batching server on the resident
-    table: 90% uniform cubes, 9% uniform cubes whose optimal length is >= 18, 1% superflips."""
-
-    from cuda_cube_solver import serving, workloads
-
-    n = args.serve
-    rng = np.random.default_rng(3)
-    pool = workloads.uniform_cubes(n + 200, seed=30)
-    hard_pool = workloads.uniform_cubes(4 * n // 10 + 16, seed=31)
-    lengths = [len(s.moves) for s in solver.solve(hard_pool)]  # set-up: find the long ones
-    hard = [c for c, L in zip(hard_pool, lengths) if L >= 18]
-    kinds_ = rng.choice(3, size=n, p=[0.90, 0.09, 0.01])
-    cubes, hi, ui = [], 0, 0
-    for k in kinds_:
-        if k == 2:
-            cubes.append(workloads.superflip())
-        elif k == 1 and hi < len(hard):
-            cubes.append(hard[hi])
-            hi += 1
-        else:
-            cubes.append(pool[ui])
-            ui += 1
-    arrivals = serving.poisson_arrivals(n, args.serve_rate, seed=3)
-    srv = serving.Server(solver.handle, 1024, opts, flip_rule=solver.flip_rule if solver.second_kind else None)
-    try:
-        stats = serving.replay(srv, cubes, arrivals)
-    finally:
-        srv.close()
-    results = stats.pop("results")
-    from cuda_cube_solver.solver import verify_solutions
-    from cuda_cube_solver.device import state_words
-
-    assert verify_solutions(state_words(cubes), [r.moves for r in results])
-    # the same cubes in one batched solve (untimed): every served length must equal it
-    batched = [len(sol.moves) for sol in solver.solve(cubes)]
-    lat = np.array([r.latency_s for r in results])
-    per_kind = {}
-    for code, name in ((0, "uniform"), (1, "length_ge_18"), (2, "superflip")):
-        sel = lat[kinds_ == code]
-        if len(sel):
-            per_kind[name] = {"p50_s": float(np.percentile(sel, 50)), "p95_s": float(np.percentile(sel, 95)),
-                              "max_s": float(sel.max())}
-    stats.update({"lengths_equal_to_batched": [r.length for r in results] == batched, "latency_by_kind": per_kind,
-                  "slots": 1024, "search_state_bytes": 1024 * (416 + 5 * 8),
-                  "mix": {"uniform": int((kinds_ == 0).sum()), "length_ge_18": int((kinds_ == 1).sum()),
-                          "superflip": int((kinds_ == 2).sum())},
-                  "rate_per_s": args.serve_rate, "table": config_table(args),
-                  "second_table": solver.second_kind, "flip_rule": solver.flip_rule if solver.second_kind else None})
-    return stats
 
 
-def batched_mix(args, solver, opts) -> dict:
-    """Config 4: one batch of ``--batch`` cubes in which 5% are hard positions -- uniform cubes of
-    seed 20 whose optimal length is >= 19 (found by set-up solves) and the superflip -- solved on
-    d4t and, with the second table attached, on d4.  Device time of each batch; the two tables
-    must give the same optimal lengths."""
-
-    from cuda_cube_solver import workloads
-    from cuda_cube_solver.device import state_words
-
-    n = args.batch
-    n_hard = max(2, n * 5 // 100)
-    cubes = workloads.uniform_cubes(n, seed=args.seed + 500)
-    cand = workloads.uniform_cubes(n_hard * 40, seed=20)
-    lengths = [len(sol.moves) for sol in solver.solve(cand)]  # set-up: find the long ones
-    hard = [c for c, L in zip(cand, lengths) if L >= 19][: n_hard - 1] + [workloads.superflip()]
-    where = np.random.default_rng(4).choice(n, size=len(hard), replace=False)
-    for i, c in zip(where, hard):
-        cubes[int(i)] = c
-    words = state_words(cubes)
-    out = {"cubes": n, "hard": len(hard), "length_ge_19": len(hard) - 1, "superflip": 1}
-    runs = [("d4t", 0)] + ([(solver.second_kind, 1)] if solver.second_kind else [])
-    lens = {}
-    for name, tid in runs:
-        res = solver.handle.solve(words, opts, np.full(n, tid, np.uint8))
-        ms, probes, _ = solver.handle.last_solve_stats()
-        lens[name] = [r.length for r in res]
-        out[name] = {"cubes_per_s": n / (ms / 1000.0), "probes_per_s": probes / (ms / 1000.0), "ms": ms}
-    if len(lens) == 2:
-        out["lengths_equal"] = lens["d4t"] == lens[solver.second_kind]
-    return out
+# ---------------------------------------------------------------------------------------------
+# the reference's own GPU build (baseline/ref_gpu.py: its kernels.cu, unmodified, its host loop)
 
 
-def build_report(args, solver, peaks) -> dict:
-    """The table build of the set-up (GPU BFS + encoding): entries per second and the
-    algorithmic DRAM write bandwidth (one depth byte per entry, then the encoded table)."""
+def reference_table(kind: str, fmt: str, device: int) -> tuple[np.ndarray, float]:
+    """The solving table built by the reference's own BFS kernels on this GPU, copied to the host."""
 
-    from cuda_cube_solver import native
+    sys.path.insert(0, str(ROOT / "baseline"))
+    import ref_gpu
 
-    nec, entries = native.kind_info(args.kind)
-    table_bytes = solver.handle.table_bytes()
-    secs = solver.build_seconds
-    written = entries + table_bytes
-    return {"kind": args.kind, "format": args.format, "gpu_seconds": secs, "entries": entries,
-            "entries_per_s": entries / secs, "table_bytes": table_bytes,
-            "write_gb_s": written / secs / 1e9, "write_frac_of_hbm": written / secs / 1e9 / float(peaks["hbm_gbs"]),
-            "depth_counts": solver.build_counts}
-
-
-def config_table(args) -> str:
-    return args.kind if args.format == "block" else f"{args.kind}-b3"
+    drv = ref_gpu.Driver(device)
+    tables = ref_gpu.RefTables(drv, kind)
+    ptr, nbytes, _, secs = tables.build(fmt)
+    host = np.empty(nbytes, np.uint8)
+    drv.d2h(host, ptr)
+    drv.free(ptr)
+    return host, secs
 
 
-def reference_gpu_arm(args, states, config) -> dict:
-    """The reference's own kernels.cu on this GPU (baseline/ref_gpu.py): its table build and its
-    per-bound host loop, the same cubes in chunks of ``--ref-batch`` (its CLI default is 100)."""
+def reference_gpu_run(kind: str, fmt: str, states, batch: int, device: int) -> dict:
+    """The reference's kernels.cu on this GPU with its per-bound host loop, ``batch`` cubes per
+    solve call (its CLI default is 100); wall clock, like the reference's own benchmark."""
 
     sys.path.insert(0, str(ROOT / "baseline"))
     import ref_gpu
 
     if not ref_gpu.available():
-        return {"impl": "reference-gpu", "unavailable": "baseline/_ref cubins not built (needs the reference checkout)"}
-    drv = ref_gpu.Driver(int(os.environ.get("LOCAL_RANK", "0")))
-    tables = ref_gpu.RefTables(drv, args.kind)
-    ptr, _, counts, build_s = tables.build(args.format)
-    solver = ref_gpu.RefSolver(drv, tables, ptr, args.format)
-    n = args.batch * args.steps
-    work = states[args.batch * args.warmup: args.batch * args.warmup + n]
-    solver.solve(states[: args.ref_batch])  # warm-up
+        return {"unavailable": "baseline/_ref cubins not built (needs the reference checkout at build time)"}
+    drv = ref_gpu.Driver(device)
+    tables = ref_gpu.RefTables(drv, kind)
+    ptr, _, _, build_s = tables.build(fmt)
+    solver = ref_gpu.RefSolver(drv, tables, ptr, fmt)
+    solver.solve(states[:batch])  # warm-up
     t0 = time.perf_counter()
-    nodes = 0
-    lengths = []
-    for i in range(0, n, args.ref_batch):
-        for moves, nd, _ in solver.solve(work[i:i + args.ref_batch]):
+    nodes, lengths = 0, []
+    for i in range(0, len(states), batch):
+        for moves, nd, _ in solver.solve(states[i:i + batch]):
             nodes += nd
             lengths.append(len(moves))
     dt = time.perf_counter() - t0
-    return {"metric": METRIC, "value": n / dt, "unit": "cubes/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 * dt / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u8/u32 integer", "data": "synthetic", "config": config,
-            "impl": "reference-gpu", "nodes_per_cube": nodes / n, "table_build_s": build_s,
-            "lengths_histogram": {str(k): lengths.count(k) for k in sorted(set(lengths))},
-            "note": f"reference kernels.cu (unmodified, nvcc sm_100) driven with its host loop, {args.ref_batch} cubes "
-                    "per solve call, wall clock including its per-bound host round trips"}
+    drv.free(ptr)
+    return {"cubes": len(states), "cubes_per_s": len(states) / dt, "seconds": dt, "batch": batch,
+            "nodes_per_cube": nodes / len(states), "table_build_s": build_s, "lengths": lengths,
+            "note": f"reference kernels.cu (unmodified, nvcc sm_100) driven with its host loop, {batch} cubes per "
+                    "solve call, wall clock including its per-bound host round trips"}
 
 
-def main() -> None:
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--batch", type=int, default=1024, help="cubes per step and rank")
-    ap.add_argument("--kind", default="d4t")
-    ap.add_argument("--format", default="block", choices=["block", "b3"])
-    ap.add_argument("--seed", type=int, default=2)
-    ap.add_argument("--impl", default="mine", choices=["mine", "reference", "reference-gpu"])
-    ap.add_argument("--ref-batch", type=int, default=100, help="reference-gpu: cubes per solve call (its CLI default)")
-    ap.add_argument("--cpu-budget", type=float, default=20.0,
-                    help="seconds of CPU work for the CPU baseline: a steady-state window with every thread busy "
-                         "(a longer run ends on its single hardest cube with the other threads idle)")
-    ap.add_argument("--plain", type=int, default=200, help="cubes solved one per call for the plain numbers")
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--variant", type=int, default=0, help="search kernel variant (libccs ccs_solve_opts.variant)")
-    ap.add_argument("--serve", type=int, default=400, help="requests in the served-stream measurement (0: skip)")
-    ap.add_argument("--tune", action="store_true", help="autotune the kernel settings on a separate sample first")
-    ap.add_argument("--serve-rate", type=float, default=100.0, help="Poisson arrival rate of the served stream (/s)")
-    ap.add_argument("--second", default=None,
-                    help="second resident table for the served stream (default: d4 beside d4t; 'none' for none)")
-    ap.add_argument("--no-ceiling", action="store_true", help="skip the random-sector gather ceiling measurement")
-    ap.add_argument("--mix", type=int, default=1, help="1: also time one batch with 5%% hard positions on d4t and d4")
-    args = ap.parse_args()
-    if args.second is None:
-        args.second = "d4" if args.kind == "d4t" and args.format == "block" else ""
-    elif args.second == "none":
-        args.second = ""
+# ---------------------------------------------------------------------------------------------
+# arms
 
-    world, rank, local = dist_setup()
+
+def reference_arm(args, world: int, rank: int, local: int) -> None:
+    """The reference's method on this host's CPU cores (rank 0 only).  Loads no libccs: the cubes
+    and frames come from the host model, the table from the reference's own kernels."""
+
+    if rank != 0:
+        return
+    from cuda_cube_solver import workloads
+
+    cubes, _ = workloads.batched_mix(args.batch, args.seed)
+    table, _ = reference_table(args.kind, args.format, local)
+    if args.warmup:  # a short warm-up window (page cache, thread start)
+        cpu_window(args.kind, args.format, table, cubes[:64], min(2.0, args.cpu_step_s))
+    cpu = cpu_window(args.kind, args.format, table, cubes[:1024], args.cpu_step_s * args.steps)
+    assert "cuda_cube_solver.native" not in sys.modules, "the reference arm must not load libccs"
+    out = {"metric": METRIC, "value": cpu["value"], "unit": "cubes/s", "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1000.0 * cpu["window_s"] / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "u8/u32 integer", "data": "synthetic",
+           "config": workload_config(args, 1), "impl": "reference",
+           "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+           "e2e": {"value": cpu["value"], "unit": "cubes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "finished": cpu["finished"], "window_s": cpu["window_s"],
+           "note": "each step is a time slice of one window over the workload's cubes; table from the reference's "
+                   "own BFS kernels (baseline/ref_gpu.py) on this GPU",
+           "reference_cpu_gather": reference_cpu_gather(None)}
+    print(json.dumps(out))
+
+
+def served_stream(args, solver, opts, rates) -> dict:
+    """The served stream: Poisson arrivals (seed 3) into the continuous-batching server on the
+    resident d4t and d4 tables (flip-count rule), 90% uniform cubes, 9% uniform cubes whose
+    optimal length is >= 18, 1% superflips; admission within a stated device-memory budget."""
+
+    from cuda_cube_solver import native, serving, workloads
+    from cuda_cube_solver.device import state_words
+    from cuda_cube_solver.solver import verify_solutions
+
+    n_max = int(max(rates) * args.serve_s)
+    pool = workloads.uniform_cubes(n_max + 64, seed=30)
+    hard_pool = workloads.uniform_cubes(n_max // 5 + 64, seed=31)
+    hard = [c for c, sol in zip(hard_pool, solver.solve(hard_pool)) if len(sol.moves) >= 18]  # set-up
+    out = {"rates": {}, "budget_bytes": args.serve_budget, "table": config_table(args),
+           "second_table": solver.second_kind, "flip_rule": solver.flip_rule if solver.second_kind else None,
+           "mix": "90% uniform, 9% uniform of optimal length >= 18, 1% superflip (seed 3)"}
+    for rate in rates:
+        n = int(rate * args.serve_s)
+        rng = np.random.default_rng(3)
+        kinds_ = rng.choice(3, size=n, p=[0.90, 0.09, 0.01])
+        cubes, hi, ui = [], 0, 0
+        for k in kinds_:
+            if k == 2:
+                cubes.append(workloads.superflip())
+            elif k == 1 and hi < len(hard):
+                cubes.append(hard[hi])
+                hi += 1
+            else:
+                cubes.append(pool[ui])
+                ui += 1
+        arrivals = serving.poisson_arrivals(n, rate, seed=3)
+        srv = serving.Server(solver.handle, opts=native.solve_opts(variant=args.serve_variant, steal=opts.steal,
+                                                                   steal_depth=opts.steal_depth),
+                             flip_rule=solver.flip_rule if solver.second_kind else None,
+                             budget_bytes=args.serve_budget)
+        try:
+            stats = serving.replay(srv, cubes, arrivals)
+            stats["memory"] = srv.memory()
+        finally:
+            srv.close()
+        results = stats.pop("results")
+        assert verify_solutions(state_words(cubes), [r.moves for r in results])
+        batched = [len(sol.moves) for sol in solver.solve(cubes)]  # untimed: the same cubes batched
+        lat = np.array([r.latency_s for r in results])
+        per_kind = {}
+        for code, name in ((0, "uniform"), (1, "length_ge_18"), (2, "superflip")):
+            sel = lat[kinds_ == code]
+            if len(sel):
+                per_kind[name] = {"n": int(len(sel)), "p50_s": float(np.percentile(sel, 50)),
+                                  "p95_s": float(np.percentile(sel, 95)), "max_s": float(sel.max())}
+        stats.update({"lengths_equal_to_batched": [r.length for r in results] == batched,
+                      "latency_by_kind": per_kind})
+        out["rates"][str(rate)] = stats
+    return out
+
+
+def main_arm(args, world: int, rank: int, local: int) -> None:
     from cuda_cube_solver import native, workloads
     from cuda_cube_solver.device import state_words
-    from cuda_cube_solver.solver import GpuSolver, frames
+    from cuda_cube_solver.solver import GpuSolver
 
-    n_steps_cubes = args.batch * (args.warmup + args.steps)
-    all_states = workloads.uniform_cubes(n_steps_cubes * world, seed=args.seed)
-    my_states = all_states[shard(n_steps_cubes, world, rank)]
-    config = {"workload": f"uniform random cubes (seed {args.seed}), {args.kind} {args.format} table resident in HBM, "
-                          f"{args.batch} cubes per step per GPU",
-              "table": args.kind if args.format == "block" else f"{args.kind}-b3", "batch": args.batch,
-              "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (7.8 GB table, random probes)"}
+    peaks = measured_peaks()
+    config = workload_config(args, world)
 
-    if args.impl == "reference-gpu":
-        if rank != 0:
-            return
-        print(json.dumps(reference_gpu_arm(args, my_states, config)))
-        return
-
-    if args.impl == "reference":
-        if rank != 0:
-            return
-        h = native.Handle(local)
-        h.build_table(args.kind, args.format, None, keep_resident=True)
-        table = h.table_copy()
-        h.close()
-        fr = np.stack([state_words(frames(s)).reshape(30) for s in my_states[: 4 * (os.cpu_count() or 1)]])
-        cpu = cpu_arm(args, my_states, fr, table, None)
-        out = {"metric": METRIC, "value": cpu["value"], "unit": "cubes/s", "n_gpus": 1, "steps": args.steps,
-               "warmup": args.warmup, "ms_per_step": 1000.0 * args.batch / cpu["value"] if cpu["value"] else None,
-               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/u32 integer",
-               "data": "synthetic", "config": config, "impl": "reference",
-               "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
-               "e2e": {"value": cpu["value"], "unit": "cubes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-               "reference_cpu_gather": reference_cpu_gather(cpu.get("probes_per_cube"))}
-        print(json.dumps(out))
-        return
-
-    # ---- setup (untimed): build the table on this GPU, keep it resident ----
+    # ---- set-up (untimed): the table built on this GPU and kept resident; the workload ----
     t = time.perf_counter()
     solver = GpuSolver.build_resident(args.kind, args.format, device=local)
-    build_s = time.perf_counter() - t
+    build_wall_s = time.perf_counter() - t
     h = solver.handle
-    solver.variant = args.variant
     solver.use_autotune = False
+    solver.variant = args.variant
+    cubes, known = workloads.batched_mix(args.batch, rank_seed(args.seed, rank))
     tuned = None
-    if args.tune:  # set-up: its own cubes (seed + 1000), not the timed ones
-        tuned = solver.autotune(workloads.uniform_cubes(args.batch, seed=args.seed + 1000), save=False)
+    if args.tune:  # its own cubes: uniform ones of seed + 1000 and hard ones past those of the batch
+        info = workloads.hard20()
+        n_hard = int(round(0.05 * args.batch)) - 1
+        extra = workloads.uniform_cubes(info["indices"][-1] + 1, seed=20)
+        sample = workloads.uniform_cubes(args.tune_cubes, seed=args.seed + 1000) + \
+            [extra[i] for i in info["indices"][n_hard:n_hard + args.tune_hard]]
+        tuned = solver.autotune(sample, save=False, budget_s=args.tune_budget)
     opts = solver._opts(n=args.batch)
-    batches = [state_words(my_states[i * args.batch:(i + 1) * args.batch]) for i in range(args.warmup + args.steps)]
 
-    for i in range(args.warmup):
-        h.solve(batches[i], opts)
+    for _ in range(args.warmup):
+        solver.solve(cubes)
 
-    # ---- timed: K batched steps, device time of the search launches ----
+    # ---- timed: K batched steps through GpuSolver.solve ----
     barrier(world)
-    kernel_ms, probes, launches, wall = [], [], [], []
+    kernel_ms, probes, launches, wall, donated = [], [], [], [], []
+    lengths = None
     with ClockSampler(local) as clocks:
-        t_all = time.perf_counter()
-        for i in range(args.warmup, args.warmup + args.steps):
+        for _ in range(args.steps):
             t0 = time.perf_counter()
-            res = h.solve(batches[i], opts)
+            sols = solver.solve(cubes)
             wall.append(time.perf_counter() - t0)
             ms, pr, ln = h.last_solve_stats()
             kernel_ms.append(ms)
             probes.append(pr)
             launches.append(ln)
-            assert all(r.status == 0 for r in res)
-        t_all = time.perf_counter() - t_all
+            donated.append(h.last_solve_donations())
+            step_lengths = [len(s.moves) for s in sols]
+            assert lengths is None or step_lengths == lengths, "optimal lengths changed between steps"
+            lengths = step_lengths
     barrier(world)
+    h2d, d2h = h.last_solve_io_bytes()
     dev_s = max_over_ranks(sum(kernel_ms) / 1000.0, world, local)
+    wall_s = max_over_ranks(sum(wall), world, local)
     value = world * args.batch * args.steps / dev_s
-
-    # ---- e2e through the public API: host cubes in, verified Solutions out ----
-    barrier(world)
-    t0 = time.perf_counter()
-    for i in range(args.warmup, args.warmup + args.steps):
-        sols = solver.solve(my_states[i * args.batch:(i + 1) * args.batch])
-    e2e_s = max_over_ranks(time.perf_counter() - t0, world, local)
-    e2e = world * args.batch * args.steps / e2e_s
+    e2e = world * args.batch * args.steps / wall_s
+    hard_ok = all(lengths[i] == L for i, L in known.items())
 
     if rank != 0:
         barrier(world)
         return
 
-    # ---- plain: one cube per call (the drop-in path), per-cube latency: uniform cubes of seed 1 ----
-    plain_lat, plain_probes, plain_dev = [], 0, 0.0
-    for s in workloads.uniform_cubes(args.plain, seed=1):
-        t0 = time.perf_counter()
-        solver.solve([s])
-        plain_lat.append(time.perf_counter() - t0)
-        plain_probes += solver.last_probes
-        plain_dev += solver.last_kernel_ms / 1000.0
-    plain = None
-    if plain_lat:
-        plain = {"cubes": len(plain_lat), "workload": "uniform random cubes (seed 1), one per call",
-                 "cubes_per_s": len(plain_lat) / sum(plain_lat),
-                 "p50_s": float(np.percentile(plain_lat, 50)), "p99_s": float(np.percentile(plain_lat, 99)),
-                 "worst_s": max(plain_lat), "probes_per_s": plain_probes / plain_dev if plain_dev else None,
-                 "batched_over_plain": value / (len(plain_lat) / sum(plain_lat))}
-
-    if args.second:  # set-up: the second resident table (d4 beside d4t)
-        solver.attach_second(args.second)
-    mix = batched_mix(args, solver, opts) if args.mix else None
-    served = None
-    if args.serve:
-        served = served_stream(args, solver, opts)
-
-    peaks = measured_peaks()
     total_probes = sum(probes)
     achieved = total_probes * SECTOR / (sum(kernel_ms) / 1000.0) / 1e9
     peak = float(peaks["hbm_gbs"])
@@ -474,39 +423,156 @@ def main() -> None:
                 "traffic": None, "probes_per_s": total_probes / (sum(kernel_ms) / 1000.0),
                 "probes_per_cube": total_probes / (args.batch * args.steps),
                 "peak_source": "measured" if not peaks.get("fallback") else "fallback",
-                "note": "algorithmic bytes = 32-byte sector per table probe, counted on the device"}
-    if not args.no_ceiling:  # the random 32-byte sector gather ceiling of this GPU (untimed)
-        ceiling, _ = native.gather_bench(local, 8 << 30, 64)
-        roofline["random_sector_ceiling"] = {"sectors_per_s": ceiling, "gb_s": ceiling * SECTOR / 1e9,
-                                             "frac": roofline["probes_per_s"] / ceiling}
+                "note": "algorithmic bytes = one 32-byte sector per table probe, probes counted on the device; "
+                        "achieved over the search launches' CUDA-event time"}
     traffic_file = ROOT / "profiles" / "search_traffic.json"
     if traffic_file.exists():
         tr = json.loads(traffic_file.read_text())
         roofline["traffic"] = tr["dram_bytes_per_probe"] * total_probes / max(1, sum(launches))
+        roofline["traffic_source"] = tr.get("source")
+
+    # ---- after the timed region (untimed) ----
+    words = state_words(cubes)
+    h.solve(state_words(workloads.uniform_cubes(1024, seed=args.seed)), opts)
+    ms, pr, _ = h.last_solve_stats()
+    uniform = {"cubes": 1024, "workload": f"uniform random cubes (seed {args.seed}) alone",
+               "cubes_per_s": 1024 / (ms / 1e3), "probes_per_s": pr / (ms / 1e3)}
+
+    plain = None
+    plain_len = None
+    plain_states = workloads.uniform_cubes(args.plain, seed=1)
+    if args.plain:  # one cube per call through the public API
+        lat, pl_probes, pl_dev, plain_len = [], 0, 0.0, []
+        for s in plain_states:
+            t0 = time.perf_counter()
+            sol = solver.solve([s])[0]
+            lat.append(time.perf_counter() - t0)
+            pl_probes += solver.last_probes
+            pl_dev += solver.last_kernel_ms / 1000.0
+            plain_len.append(len(sol.moves))
+        rate = len(lat) / sum(lat)
+        plain = {"cubes": len(lat), "workload": "uniform random cubes (seed 1), one per GpuSolver.solve call",
+                 "cubes_per_s": rate, "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                 "worst_s": max(lat), "probes_per_s": pl_probes / pl_dev if pl_dev else None,
+                 "batched_over_plain": value / rate, "e2e_batched_over_plain": e2e / rate,
+                 "uniform_batched_over_plain": uniform["cubes_per_s"] / rate}
+
+    ref_gpu = None
+    if args.ref_gpu and args.plain:
+        ref_gpu = reference_gpu_run(args.kind, args.format, plain_states, args.ref_batch, local)
+        if "lengths" in ref_gpu:
+            ref_gpu["lengths_equal_to_plain"] = ref_gpu.pop("lengths") == plain_len
+            ref_gpu["ours_over_reference"] = {"batched": value / ref_gpu["cubes_per_s"],
+                                              "e2e": e2e / ref_gpu["cubes_per_s"],
+                                              "plain": plain["cubes_per_s"] / ref_gpu["cubes_per_s"]}
+
+    # the same batch on d4 (second resident table) and with the flip-count rule
+    mix = {config_table(args): {"cubes_per_s": value, "probes_per_s": roofline["probes_per_s"],
+                                "hard_lengths_equal_to_known": hard_ok}}
+    if args.second:
+        solver.attach_second(args.second)
+        res = h.solve(words, opts, np.ones(len(words), np.uint8))
+        ms, pr, _ = h.last_solve_stats()
+        mix[args.second] = {"cubes_per_s": args.batch / (ms / 1e3), "probes_per_s": pr / (ms / 1e3),
+                            "lengths_equal": [r.length for r in res] == lengths}
+        solver.solve(cubes)
+        ms, pr, _ = h.last_solve_stats()
+        mix["flip_rule"] = {"rule": f">= {solver.flip_rule} flipped edges -> {args.second}",
+                            "cubes_per_s": args.batch / (ms / 1e3), "probes_per_s": pr / (ms / 1e3)}
+
+    served = None
+    if args.serve_s > 0:
+        served = served_stream(args, solver, opts, [float(r) for r in args.serve_rates.split(",")])
+        if plain:
+            for st in served["rates"].values():
+                st["sustained_over_plain"] = st["sustained_per_s"] / plain["cubes_per_s"]
+
+    if not args.no_ceiling:  # the random 32-byte sector gather ceiling of this GPU
+        ceiling, _ = native.gather_bench(local, 8 << 30, 64)
+        roofline["random_sector_ceiling"] = {"sectors_per_s": ceiling, "gb_s": ceiling * SECTOR / 1e9,
+                                             "frac": roofline["probes_per_s"] / ceiling}
 
     cpu = None
     if not args.no_cpu:
-        table = h.table_copy()
-        fr = np.stack([state_words(frames(s)).reshape(30) for s in my_states[: 4 * (os.cpu_count() or 1)]])
-        cpu = cpu_arm(args, my_states, fr, table, roofline["probes_per_cube"])
-        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        c = cpu_window(args.kind, args.format, h.table_copy(), cubes[:1024], args.cpu_budget)
+        cpu = {k: c[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cpu["reference_cpu_gather"] = reference_cpu_gather(roofline["probes_per_cube"])
 
+    _, entries = native.kind_info(args.kind)
     out = {"metric": METRIC, "value": value, "unit": "cubes/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": 1000.0 * dev_s / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "u8/u32 integer", "data": "synthetic",
            "config": config,
-           "e2e": {"value": e2e, "unit": "cubes/s", "h2d_bytes_per_step": 20 * args.batch,
-                   "d2h_bytes_per_step": native.ctypes.sizeof(native.Result) * args.batch},
+           "e2e": {"value": e2e, "unit": "cubes/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                   "api": "GpuSolver.solve (host CubieState list in, verified Solution list out)"},
            "gpu_launches": int(sum(launches)),
            "kernel_settings": {"variant": opts.variant, "base_plen": opts.base_plen, "spread": opts.spread,
                                "move_min": opts.move_min, "move_age": opts.move_age, "probe_min": opts.probe_min,
-                               "autotuned": tuned is not None},
+                               "steal": opts.steal, "steal_depth": opts.steal_depth, "autotuned": tuned is not None,
+                               "tuning": {k: tuned[k] for k in ("cubes_per_s", "default_cubes_per_s", "trials",
+                                                                 "complete", "seconds", "sample")} if tuned else None},
+           "donated_subtrees_per_step": statistics.mean(donated),
+           "lengths": {"histogram": {str(k): lengths.count(k) for k in sorted(set(lengths))},
+                       "hard_equal_to_known": hard_ok, "equal_across_steps": True},
            "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
-           "plain": plain, "batched_mix": mix, "served": served, "table_build_s": build_s, "table_build_gpu_s": solver.build_seconds,
-           "table_build": build_report(args, solver, peaks),
+           "batched_mix": mix, "uniform_1024": uniform, "plain": plain, "reference_gpu": ref_gpu, "served": served,
+           "table_build": {"kind": args.kind, "format": args.format, "gpu_seconds": solver.build_seconds,
+                           "wall_s": build_wall_s, "entries": entries, "entries_per_s": entries / solver.build_seconds,
+                           "table_bytes": h.table_bytes(), "depth_counts": solver.build_counts},
            "wall_s_per_step": statistics.mean(wall)}
     print(json.dumps(out))
     barrier(world)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=4096, help="cubes per step and rank (5%% of them hard)")
+    ap.add_argument("--kind", default="d4t")
+    ap.add_argument("--format", default="block", choices=["block", "b3"])
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference", "reference-gpu"])
+    ap.add_argument("--variant", type=int, default=0, help="search kernel variant (ccs_solve_opts.variant)")
+    ap.add_argument("--no-tune", dest="tune", action="store_false", help="skip the autotuner (library defaults)")
+    ap.add_argument("--tune-budget", type=float, default=90.0, help="seconds of autotuning at most")
+    ap.add_argument("--tune-cubes", type=int, default=512)
+    ap.add_argument("--tune-hard", type=int, default=8)
+    ap.add_argument("--plain", type=int, default=1000, help="cubes solved one per call (0: skip)")
+    ap.add_argument("--ref-gpu", type=int, default=1, help="1: time the reference's kernels.cu on the plain cubes")
+    ap.add_argument("--ref-batch", type=int, default=100, help="reference kernels: cubes per solve call (its default)")
+    ap.add_argument("--second", default="d4", help="second resident table for the d4 leg and serving ('' for none)")
+    ap.add_argument("--serve-s", type=float, default=8.0, help="seconds of arrivals per served rate (0: skip)")
+    ap.add_argument("--serve-rates", default="10,50,100,200")
+    ap.add_argument("--serve-variant", type=int, default=0, help="server kernel variant (0: automatic)")
+    ap.add_argument("--serve-budget", type=int, default=16 << 30,
+                    help="device-memory budget of the served stream in bytes (tables, search state, stacks)")
+    ap.add_argument("--no-ceiling", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of the CPU baseline window")
+    ap.add_argument("--cpu-step-s", type=float, default=6.0, help="reference arm: seconds of CPU work per step")
+    args = ap.parse_args()
+    if args.format != "block" or args.kind != "d4t":
+        args.second = ""  # (d4 beside d4t is the configuration's pair)
+
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        reference_arm(args, world, rank, local)
+        return
+    if args.impl == "reference-gpu":
+        if rank != 0:
+            return
+        from cuda_cube_solver import workloads
+
+        states = workloads.uniform_cubes(args.plain or 1000, seed=1)
+        r = reference_gpu_run(args.kind, args.format, states, args.ref_batch, local)
+        r.pop("lengths", None)
+        print(json.dumps({"metric": METRIC, "value": r.get("cubes_per_s"), "unit": "cubes/s", "n_gpus": 1,
+                          "impl": "reference-gpu", "config": {"workload": f"{len(states)} uniform random cubes "
+                                                                          "(seed 1), the plain drop-in set"}, **r}))
+        return
+    main_arm(args, world, rank, local)
 
 
 if __name__ == "__main__":
