@@ -158,14 +158,29 @@ __device__ __forceinline__ uint64_t table_index_dev(const DevTables& T, const ui
 
 // The whole 32-byte sector of a probe in one 256-bit load: one sector request instead of two
 // (the minimum and the offset word travel separately otherwise).  The table is read-only while
-// searching, so the load may be scheduled freely.
+// searching, so the load may be scheduled freely.  Measured on B200 with random sectors of an
+// 8 GB buffer (ncu): a plain ld.global.nc moves 129 DRAM bytes per 32-byte sector and 4.5 L2
+// sectors per load; the .L2::64B size hint halves both (68 B, 2.5) and raises the random-sector
+// rate by 8%; .L1::no_allocate keeps these never-reused sectors out of L1 (the corner classes and
+// the lanes' stacks use it).  CCS_SECTOR_LOAD_FORM: 0 plain, 1 .L2::64B, 2 both (default).
+#ifndef CCS_SECTOR_LOAD_FORM
+#define CCS_SECTOR_LOAD_FORM 2
+#endif
 __device__ __forceinline__ void load_sector(const uint32_t* p, uint32_t w[8]) {
 #ifdef CCS_HOST_EMULATION  // host build of this header for the CPU tests
     for (int i = 0; i < 8; ++i) w[i] = p[i];
 #else
-    asm("ld.global.nc.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+#if CCS_SECTOR_LOAD_FORM == 0
+#define CCS_LD_SECTOR "ld.global.nc.v8.u32"
+#elif CCS_SECTOR_LOAD_FORM == 1
+#define CCS_LD_SECTOR "ld.global.nc.L2::64B.v8.u32"
+#else
+#define CCS_LD_SECTOR "ld.global.nc.L1::no_allocate.L2::64B.v8.u32"
+#endif
+    asm(CCS_LD_SECTOR " {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
         : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7])
         : "l"(p));
+#undef CCS_LD_SECTOR
 #endif
 }
 

@@ -125,9 +125,12 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                                    ~((2u << mm) - 1u);
                             ord = frame_order(h, bound - (uint32_t)g);
                         }
-                        if (STEAL && ((cut >> g) & 1u)) {  // this node's remaining children were donated
-                            todo = 0u;
-                            cut &= ~(1u << g);
+                        if (STEAL) {
+                            cut &= (2u << g) - 1u;  // nodes below this one are gone: their marks too
+                            if ((cut >> g) & 1u) {  // this node's remaining children were donated
+                                todo = 0u;
+                                cut &= ~(1u << g);
+                            }
                         }
                         if (LOOKAHEAD && ((stash >> g) & 1u)) {  // the stashed sibling resumes
                             stash &= ~(1u << g);
@@ -277,8 +280,10 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                                                   ((unsigned long long)bound << 37) | ((unsigned long long)rest << 42);
                     atomicAdd(&P.slots[slot].open, 1u);  // before the post: the count never runs short
                     if (post_donation(P, lane_seed + don_tick, slot, w1, w2, w3)) {
+                        // the donated children are skipped here: now, and when a pop returns to
+                        // this node (a pop recomputes a node's remaining children from its path)
                         if (l == g) todo = 0u;
-                        else cut |= 1u << l;
+                        cut |= 1u << l;
                     } else {
                         atomicSub(&P.slots[slot].open, 1u);  // (this lane's own unit keeps it above 0)
                     }
