@@ -35,10 +35,11 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lane_seed = (blockIdx.x * blockDim.x + threadIdx.x) * 0x9E3779B1u >> 7;
 
-    // Work stealing (not with LOOKAHEAD, whose stash holds siblings the donation would repeat):
-    // gbase = depth of the lane's unit root (0 for an item, the donated node's depth for a donated
-    // subtree); bit l of `cut` = the remaining children of the node at depth l were donated.
-    constexpr bool STEAL = !LOOKAHEAD;
+    // Work stealing: gbase = depth of the lane's unit root (0 for an item, the donated node's depth
+    // for a donated subtree); bit l of `cut` = the remaining children of the node at depth l were
+    // donated.  With LOOKAHEAD a sibling stashed at depth l stays with the donor (it resumes there
+    // when the subtree pops back) and is left out of the donation.
+    constexpr bool STEAL = true;
     int gbase = 0;
     uint32_t cut = 0, don_tick = 0;
     int mv = 0;  // frame update this lane waits for: 0 none, 1 push child m, 2 pop one level
@@ -269,6 +270,7 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                         const int last = l > 0 ? path[l - 1] : -1;
                         rest = T.amask[last + 1] & ~axis_move_mask(excluded_axes(hl, bound - (uint32_t)l)) &
                                ~((2u << path[l]) - 1u);
+                        if (LOOKAHEAD && ((stash >> l) & 1u)) rest &= ~(1u << ((la_x[l] >> 18) & 31u));
                     }
                     if (!rest) continue;
                     unsigned long long w2 = 0, w3 = 0;

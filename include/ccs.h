@@ -128,7 +128,7 @@ typedef struct ccs_solve_opts {
     int probe_min;            /* a warp keeps probing (pruned children -> next sibling) while  */
                               /*   at least this many lanes have a probe (0: default, > 32: off) */
     int steal;                /* work stealing: lanes donate unexplored subtrees to idle lanes  */
-                              /*   (variants 1, 3, 6, 7; 0: on, < 0: off)                       */
+                              /*   (phase-ordered variants 1-3, 6, 7; 0: on, < 0: off)          */
     int steal_depth;          /* a donated subtree has at least this many moves to the bound (0: 6) */
 } ccs_solve_opts;
 

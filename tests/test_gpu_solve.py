@@ -96,17 +96,19 @@ def test_illegal_state_is_rejected():
         h.solve(bad)
 
 
-def test_work_stealing_keeps_lengths_and_iteration_nodes(lengths_golden):
+@pytest.mark.parametrize("variant", [1, 2], ids=["throughput", "lookahead"])
+def test_work_stealing_keeps_lengths_and_iteration_nodes(lengths_golden, variant):
     """Donated subtrees are searched exactly once: with stealing on (and forced often by a small
     minimum depth) every completed iteration has the same node count as without it, the lengths
-    equal the reference's, and subtrees were in fact donated."""
+    equal the reference's, and subtrees were in fact donated (also by the lookahead kernel, whose
+    stashed siblings stay with the donor)."""
 
     h = resident_handle("d4")
     # fewer than 32 cubes and no deeper prefixes: prefix lengths then do not depend on timing
     cubes = lengths_golden["distance20"][:4] + [lengths_golden["hard19"]] + lengths_golden["random1000"][:26]
     states = [_state(parse_moves(c["scramble"])) for c in cubes]
     words = state_words(states)
-    base = dict(timeout_s=900, variant=1, deeper_at=(1e18, 1e18))
+    base = dict(timeout_s=900, variant=variant, deeper_at=(1e18, 1e18))
     off = h.solve(words, native.solve_opts(steal=-1, **base))
     assert h.last_solve_donations() == 0
     for depth in (6, 3):
