@@ -25,7 +25,8 @@ struct BfsParams {
     const uint32_t* classidx;
     const uint32_t* class_rep;
     const uint16_t* class_stab;
-    unsigned long long* counter;     // entries found in this pass
+    unsigned long long* counter;     // [0] entries found in this pass, [1] random depth-byte reads,
+                                     // [2] claim attempts (atomics), for the pass's roofline
 };
 
 __device__ __forceinline__ uint32_t claim_entry(uint8_t* depth, uint64_t idx, uint32_t d1) {
@@ -58,6 +59,16 @@ __device__ __forceinline__ void add_count(unsigned long long* counter, unsigned 
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xFFFFFFFFu, local, o);
     if ((threadIdx.x & 31u) == 0 && local) atomicAdd(counter, local);
+}
+
+// Claims that found the byte unvisited (the atomic's return tells) and attempts, counted apart.
+__device__ __forceinline__ uint32_t claim_counted(uint8_t* depth, uint64_t idx, uint32_t d1, uint32_t& attempts) {
+    if (((volatile uint8_t*)depth)[idx] != 0xFFu) return 0;
+    ++attempts;
+    uint32_t* w = reinterpret_cast<uint32_t*>(depth + (idx & ~3ull));
+    uint32_t sh = (uint32_t)(idx & 3u) * 8u;
+    uint32_t old = atomicAnd(w, ~(0xFFu << sh) | (d1 << sh));
+    return ((old >> sh) & 0xFFu) == 0xFFu;
 }
 
 template <int MODE, int NEC>
@@ -109,6 +120,7 @@ __global__ void __launch_bounds__(256) bfs_forward(const DevTables* __restrict__
     stage_tables(T, gT);
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     unsigned long long local = 0;
+    uint32_t reads = 0, attempts = 0;
     const uint8_t* depth = P.depth;
     const uint32_t d1 = d + 1u;
     const uint64_t n_groups = (P.n_chunks + 31u) / 32u;
@@ -141,17 +153,19 @@ __global__ void __launch_bounds__(256) bfs_forward(const DevTables* __restrict__
                 uint32_t b[3];
 #pragma unroll
                 for (int i = 0; i < 3; ++i) b[i] = depth[j[i]];  // a stale 0xFF is settled by the atomic
+                reads += 3u;
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
-                    if (stab[i] && b[i] == 0xFFu) local += claim_entry(P.depth, j[i], d1);
+                    if (stab[i] && b[i] == 0xFFu) local += claim_counted(P.depth, j[i], d1, attempts);
                     uint32_t rest = stab[i] & (stab[i] - 1);  // the other stabiliser images
                     while (rest) {
                         const uint32_t t = __ffs(rest) - 1;
                         rest &= rest - 1;
-                        local += claim_entry(P.depth,
-                                             (uint64_t)(packed[i] >> 4) * KindTraits<MODE, NEC>::N_EDGE +
-                                                 edge_coord_sym<MODE, NEC>(T, n[i], T.sym_mul[t][packed[i] & 15u]),
-                                             d1);
+                        ++reads;
+                        local += claim_counted(P.depth,
+                                               (uint64_t)(packed[i] >> 4) * KindTraits<MODE, NEC>::N_EDGE +
+                                                   edge_coord_sym<MODE, NEC>(T, n[i], T.sym_mul[t][packed[i] & 15u]),
+                                               d1, attempts);
                     }
                 }
             }
@@ -159,6 +173,8 @@ __global__ void __launch_bounds__(256) bfs_forward(const DevTables* __restrict__
         __syncwarp();
     }
     add_count(P.counter, local);
+    add_count(P.counter + 1, reads);
+    add_count(P.counter + 2, attempts);
 }
 
 // Backward pass: an unvisited entry with a neighbour at depth d is at depth d + 1.  A warp takes
@@ -175,6 +191,7 @@ __global__ void __launch_bounds__(256) bfs_backward(const DevTables* __restrict_
     stage_tables(T, gT);
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     unsigned long long local = 0;
+    uint32_t reads = 0;
     const uint8_t* depth = P.depth;
     const uint64_t n_groups = (P.n_chunks + 31u) / 32u;
     const uint64_t n_warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
@@ -195,6 +212,7 @@ __global__ void __launch_bounds__(256) bfs_backward(const DevTables* __restrict_
                 const uint64_t j1 = table_index_dev<MODE, NEC>(T, P.classidx, n1);
                 const uint64_t j2 = table_index_dev<MODE, NEC>(T, P.classidx, n2);
                 const uint32_t b0 = depth[j0], b1 = depth[j1], b2 = depth[j2];
+                reads += 3u;
                 found = b0 == d || b1 == d || b2 == d;
             }
             if (found) {
@@ -205,6 +223,7 @@ __global__ void __launch_bounds__(256) bfs_backward(const DevTables* __restrict_
         __syncwarp();
     }
     add_count(P.counter, local);
+    add_count(P.counter + 1, reads);
 }
 
 // Histogram of depth values (0..31, plus unvisited in bin 32).

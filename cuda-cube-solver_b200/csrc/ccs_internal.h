@@ -100,6 +100,7 @@ struct ccs_handle {
     uint64_t last_h2d = 0, last_d2h = 0;
     int last_launches = 0;
     ccs::Server* server = nullptr;
+    std::vector<ccs_bfs_pass> last_passes;  // the last table build's BFS passes
 };
 
 namespace ccs {

@@ -201,6 +201,14 @@ extern "C" int ccs_attach_table(ccs_handle* h, const char* kind, int format, con
     return rc;
 }
 
+extern "C" int ccs_last_build_passes(ccs_handle* h, ccs_bfs_pass* out, int max_out, int* n_out) {
+    if (!h || !n_out || (max_out > 0 && !out)) return fail(CCS_E_ARG, "NULL argument");
+    int n = (int)h->last_passes.size();
+    for (int i = 0; i < n && i < max_out; ++i) out[i] = h->last_passes[i];
+    *n_out = n;
+    return CCS_OK;
+}
+
 extern "C" int ccs_build_table(ccs_handle* h, const char* kind, int format, const char* out_path, int keep_resident,
                                uint64_t* depth_counts, int max_depths, int* n_depths, double* seconds,
                                ccs_log_fn log) {
@@ -241,6 +249,33 @@ extern "C" int ccs_build_table(ccs_handle* h, const char* kind, int format, cons
         CCS_CUDA_TRY(cudaMemsetAsync(counter.p, 0, 8, h->stream));
         return CCS_OK;
     };
+    // per pass: entries found, random depth-byte reads, claim attempts, device time
+    h->last_passes.clear();
+    cudaEvent_t pe0, pe1;
+    CCS_CUDA_TRY(cudaEventCreate(&pe0));
+    CCS_CUDA_TRY(cudaEventCreate(&pe1));
+    struct EventPair {
+        cudaEvent_t a, b;
+        ~EventPair() { cudaEventDestroy(a); cudaEventDestroy(b); }
+    } ev_guard{pe0, pe1};
+    auto read_pass = [&](uint32_t d, bool fwd, uint64_t* found) -> int {
+        unsigned long long c[3];
+        CCS_CUDA_TRY(cudaMemcpyAsync(c, counter.p, sizeof c, cudaMemcpyDeviceToHost, h->stream));
+        CCS_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        CCS_CUDA_TRY(cudaMemsetAsync(counter.p, 0, sizeof c, h->stream));
+        float ms = 0;
+        CCS_CUDA_TRY(cudaEventElapsedTime(&ms, pe0, pe1));
+        ccs_bfs_pass rec{};
+        rec.depth = (int32_t)d + 1;
+        rec.forward = fwd ? 1 : 0;
+        rec.found = c[0];
+        rec.random_reads = c[1];
+        rec.claims = c[2];
+        rec.seconds = ms * 1e-3;
+        h->last_passes.push_back(rec);
+        *found = c[0];
+        return CCS_OK;
+    };
     CCS_TRY(dispatch_kind(k, [&](auto M, auto N) {
         constexpr int MODE = decltype(M)::value, NEC = decltype(N)::value;
         bfs_seed<MODE, NEC><<<1, 32, 0, h->stream>>>(h->d_tables, P);
@@ -255,10 +290,12 @@ extern "C" int ccs_build_table(ccs_handle* h, const char* kind, int format, cons
             // quarter of the unvisited entries, backward afterwards.
             bool forward = counts.back() < remaining / 4;
             auto ts = std::chrono::steady_clock::now();
+            CCS_CUDA_TRY(cudaEventRecord(pe0, h->stream));
             if (forward) bfs_forward<MODE, NEC><<<grid, 256, 0, h->stream>>>(h->d_tables, P, d);
             else bfs_backward<MODE, NEC><<<grid, 256, 0, h->stream>>>(h->d_tables, P, d);
             CCS_CUDA_TRY(cudaGetLastError());
-            CCS_TRY(read_counter(&found));
+            CCS_CUDA_TRY(cudaEventRecord(pe1, h->stream));
+            CCS_TRY(read_pass(d, forward, &found));
             double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count();
             log_msg(log, "depth %2u %s found %14llu (%7.2fs)", d + 1, forward ? "fwd" : "bwd", (unsigned long long)found, dt);
             if (found == 0) return fail(CCS_E_UNREACHABLE, "%llu entries unreachable", (unsigned long long)remaining);

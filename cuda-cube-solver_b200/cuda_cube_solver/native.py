@@ -66,6 +66,11 @@ class Result(ctypes.Structure):
     ]
 
 
+class BfsPass(ctypes.Structure):
+    _fields_ = [("depth", ctypes.c_int32), ("forward", ctypes.c_int32), ("found", ctypes.c_uint64),
+                ("random_reads", ctypes.c_uint64), ("claims", ctypes.c_uint64), ("seconds", ctypes.c_double)]
+
+
 LOG_FN = ctypes.CFUNCTYPE(None, ctypes.c_char_p)
 
 # name -> (argtypes); every function returns int (status) except where noted.
@@ -81,6 +86,7 @@ _SIGS = {
     "ccs_kind_tables": [ctypes.c_char_p] + [ctypes.c_void_p] * 5,
     "ccs_set_kind": [ctypes.c_void_p, ctypes.c_char_p],
     "ccs_last_solve_donations": [ctypes.c_void_p, _P(ctypes.c_uint64)],
+    "ccs_last_build_passes": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _P(ctypes.c_int)],
     "ccs_server_start_budget": [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, _P(ctypes.c_int)],
     "ccs_server_memory": [ctypes.c_void_p] + [_P(ctypes.c_uint64)] * 4,
     "ccs_last_solve_io_bytes": [ctypes.c_void_p, _P(ctypes.c_uint64), _P(ctypes.c_uint64)],
@@ -215,6 +221,15 @@ class Handle:
                                   None if out_path is None else str(out_path).encode(), int(keep_resident),
                                   _ptr(counts), 64, ctypes.byref(n), ctypes.byref(secs), cb))
         return [int(c) for c in counts[:n.value]], secs.value
+
+    def last_build_passes(self) -> list[dict]:
+        """The last build's BFS passes: depth, direction, entries found, random reads, claims, seconds."""
+
+        buf = (BfsPass * 64)()
+        n = ctypes.c_int()
+        check(lib.ccs_last_build_passes(self._h, ctypes.cast(buf, ctypes.c_void_p), 64, ctypes.byref(n)))
+        return [{"depth": p.depth, "forward": bool(p.forward), "found": p.found, "random_reads": p.random_reads,
+                 "claims": p.claims, "seconds": p.seconds} for p in buf[: n.value]]
 
     def table_bytes(self) -> int:
         n = ctypes.c_uint64()

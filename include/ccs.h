@@ -86,6 +86,21 @@ int ccs_load_table(ccs_handle* h, const char* kind, int format, const char* path
 int ccs_build_table(ccs_handle* h, const char* kind, int format, const char* out_path, int keep_resident,
                     uint64_t* depth_counts, int max_depths, int* n_depths, double* seconds, ccs_log_fn log);
 
+/* One BFS pass of the last ccs_build_table: the depth it assigned, forward (1: expand the
+ * frontier, kernels.cu:544-574) or backward (0: unvisited entries test their neighbours,
+ * kernels.cu:577-611), the entries found, the random depth-byte reads and the claim attempts
+ * (atomics) it made, and its device time.  Algorithmic bytes of a pass: one sequential scan of
+ * the depth bytes plus one 32-byte sector per random read and per claim. */
+typedef struct ccs_bfs_pass {
+    int32_t depth;
+    int32_t forward;
+    uint64_t found;
+    uint64_t random_reads;
+    uint64_t claims;
+    double seconds;
+} ccs_bfs_pass;
+int ccs_last_build_passes(ccs_handle* h, ccs_bfs_pass* out, int max_out, int* n_out);
+
 /* A second resident table (table id 1) of the same kind family and format as the first, e.g. d4
  * next to d4t: one search launch then serves cubes of either table, chosen per cube.  Loaded from
  * a file here; ccs_build_table with keep_resident = 2 builds it in place instead. */

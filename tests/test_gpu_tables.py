@@ -41,6 +41,10 @@ def test_304_counts_and_bytes(depth_golden):
     digest = _sha(h.table_copy())
     assert digest == _sha_golden()["304"]["block_sha256"]  # the CPU oracle's independent build
     assert digest == _ref_sha()["304"]["reference_sha256"]  # the reference's own kernels
+    passes = h.last_build_passes()  # per-pass counters behind the build's roofline
+    assert [p["found"] for p in passes] == h.build_counts[1:]
+    assert all(p["random_reads"] > 0 and p["seconds"] > 0 for p in passes)
+    assert any(p["forward"] and p["claims"] >= p["found"] for p in passes)
 
 
 @pytest.mark.parametrize("name", ["d4t", "d4"])
