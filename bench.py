@@ -302,6 +302,31 @@ def reference_arm(args, world: int, rank: int, local: int) -> None:
     print(json.dumps(out))
 
 
+def bfs_roofline(passes: list[dict], entries: int, peak_gbs: float, ceiling: float | None) -> dict:
+    """The table build's passes against their rooflines: algorithmic bytes of a pass = one
+    sequential scan of the depth bytes (one per entry) + one 32-byte sector per random read and
+    per claim; the random sectors also against the random-sector ceiling."""
+
+    rows = []
+    for p in passes:
+        random = p["random_reads"] + p["claims"]
+        algo = entries + SECTOR * random
+        rows.append({"depth": p["depth"], "dir": "fwd" if p["forward"] else "bwd", "found": p["found"],
+                     "random_sectors": random, "seconds": p["seconds"], "algorithmic_gb": algo / 1e9,
+                     "achieved_gb_s": algo / p["seconds"] / 1e9, "random_sectors_per_s": random / p["seconds"]})
+    total_s = sum(r["seconds"] for r in rows)
+    top = max(rows, key=lambda r: r["seconds"]) if rows else None
+    out = {"passes": rows, "bfs_seconds": total_s,
+           "dominant_pass": top and {k: top[k] for k in ("depth", "dir", "seconds")},
+           "dominant_share": top["seconds"] / total_s if top else None}
+    if top:
+        out["achieved_gb_s"] = top["achieved_gb_s"]
+        out["frac_of_hbm_peak"] = top["achieved_gb_s"] / peak_gbs
+        if ceiling:
+            out["frac_of_random_sector_ceiling"] = top["random_sectors_per_s"] / ceiling
+    return out
+
+
 def served_stream(args, solver, opts, rates) -> dict:
     """The served stream: Poisson arrivals (seed 3) into the continuous-batching server on the
     resident d4t and d4 tables (flip-count rule), 90% uniform cubes, 9% uniform cubes whose
@@ -371,6 +396,7 @@ def main_arm(args, world: int, rank: int, local: int) -> None:
     solver = GpuSolver.build_resident(args.kind, args.format, device=local)
     build_wall_s = time.perf_counter() - t
     h = solver.handle
+    build_passes = h.last_build_passes()
     solver.use_autotune = False
     solver.variant = args.variant
     cubes, known = workloads.batched_mix(args.batch, rank_seed(args.seed, rank))
@@ -487,6 +513,7 @@ def main_arm(args, world: int, rank: int, local: int) -> None:
             for st in served["rates"].values():
                 st["sustained_over_plain"] = st["sustained_per_s"] / plain["cubes_per_s"]
 
+    ceiling = None
     if not args.no_ceiling:  # the random 32-byte sector gather ceiling of this GPU
         ceiling, _ = native.gather_bench(local, 8 << 30, 64)
         roofline["random_sector_ceiling"] = {"sectors_per_s": ceiling, "gb_s": ceiling * SECTOR / 1e9,
@@ -518,7 +545,8 @@ def main_arm(args, world: int, rank: int, local: int) -> None:
            "batched_mix": mix, "uniform_1024": uniform, "plain": plain, "reference_gpu": ref_gpu, "served": served,
            "table_build": {"kind": args.kind, "format": args.format, "gpu_seconds": solver.build_seconds,
                            "wall_s": build_wall_s, "entries": entries, "entries_per_s": entries / solver.build_seconds,
-                           "table_bytes": h.table_bytes(), "depth_counts": solver.build_counts},
+                           "table_bytes": h.table_bytes(), "depth_counts": solver.build_counts,
+                           "roofline": bfs_roofline(build_passes, entries, peak, ceiling)},
            "wall_s_per_step": statistics.mean(wall)}
     print(json.dumps(out))
     barrier(world)
