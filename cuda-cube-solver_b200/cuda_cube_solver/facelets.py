@@ -12,6 +12,8 @@ grids in 3D rather than listed.
 
 from __future__ import annotations
 
+from collections import Counter
+
 from cuda_cube_solver.cubie import CORNER_NAMES, EDGE_NAMES, FACE_NORMAL, CubieState, permutation_parity
 
 FACES = "URFDLB"
@@ -66,8 +68,33 @@ def is_facelet_string(text: str) -> bool:
     return len(s) == 54 and len(set(s)) == 6
 
 
+def _piece_lookups() -> tuple[dict, dict]:
+    """What a slot shows, mapped to the piece and orientation that show it: for every corner
+    cubie and twist the three stickers read in slot order, for every edge cubie and flip the two."""
+
+    corners = {}
+    for cubie, name in enumerate(CORNER_NAMES):
+        for twist in range(3):
+            shown = [""] * 3
+            for k in range(3):
+                shown[(k + twist) % 3] = name[k]
+            corners[tuple(shown)] = (cubie, twist)
+    edges = {}
+    for cubie, name in enumerate(EDGE_NAMES):
+        edges[name] = (cubie, 0)
+        edges[name[::-1]] = (cubie, 1)
+    return corners, edges
+
+
+_CORNER_SEEN, _EDGE_SEEN = _piece_lookups()
+
+
 def parse_facelets(text: str) -> CubieState:
-    """Cubie state of a 54-sticker string; raises ``FaceletError`` if it is not a legal cube."""
+    """Cubie state of a 54-sticker string; raises ``FaceletError`` if it is not a legal cube.
+
+    Stickers are renamed by the centre they match, each slot's stickers are looked up in the table
+    of what every piece shows in every orientation, and the result must be a legal cube.  The
+    error messages are the reference's (facelets.py:44-98), which callers may match."""
 
     s = "".join(text.split())
     if len(s) != 54:
@@ -75,50 +102,41 @@ def parse_facelets(text: str) -> CubieState:
     centres = [s[4 + 9 * f] for f in range(6)]
     if len(set(centres)) != 6:
         raise FaceletError("the six centre stickers must all differ")
-    face_of = {c: FACES[f] for f, c in enumerate(centres)}
-    try:
-        faces = [face_of[c] for c in s]
-    except KeyError as exc:
-        raise FaceletError(f"sticker {exc.args[0]!r} matches no centre") from None
-    for f in FACES:
-        if faces.count(f) != 9:
-            raise FaceletError(f"face {f} has {faces.count(f)} stickers, expected 9")
+    face_of = dict(zip(centres, FACES))
+    unknown = next((c for c in s if c not in face_of), None)
+    if unknown is not None:
+        raise FaceletError(f"sticker {unknown!r} matches no centre")
+    faces = "".join(face_of[c] for c in s)
+    counts = Counter(faces)
+    short = next((f for f in FACES if counts[f] != 9), None)
+    if short is not None:
+        raise FaceletError(f"face {short} has {counts[short]} stickers, expected 9")
 
-    cp, co = [], []
+    corners = []
     for pos, slots in enumerate(CORNER_FACELETS):
-        st = [faces[i] for i in slots]
-        twist = next((k for k in range(3) if st[k] in "UD"), None)
-        if twist is None:
+        shown = tuple(faces[i] for i in slots)
+        if not set(shown) & {"U", "D"}:
             raise FaceletError(f"corner at {CORNER_NAMES[pos]} has no U or D sticker")
-        rest = (st[(twist + 1) % 3], st[(twist + 2) % 3])
-        cubie = next((j for j, nm in enumerate(CORNER_NAMES) if nm[0] == st[twist] and (nm[1], nm[2]) == rest), None)
-        if cubie is None:
-            raise FaceletError(f"corner at {CORNER_NAMES[pos]} has impossible colours {''.join(st)}")
-        cp.append(cubie)
-        co.append(twist)
-
-    ep, eo = [], []
+        if shown not in _CORNER_SEEN:
+            raise FaceletError(f"corner at {CORNER_NAMES[pos]} has impossible colours {''.join(shown)}")
+        corners.append(_CORNER_SEEN[shown])
+    edges = []
     for pos, (a, b) in enumerate(EDGE_FACELETS):
-        pair = faces[a] + faces[b]
-        if pair in EDGE_NAMES:
-            ep.append(EDGE_NAMES.index(pair))
-            eo.append(0)
-        elif pair[::-1] in EDGE_NAMES:
-            ep.append(EDGE_NAMES.index(pair[::-1]))
-            eo.append(1)
-        else:
-            raise FaceletError(f"edge at {EDGE_NAMES[pos]} has impossible colours {pair}")
+        shown = faces[a] + faces[b]
+        if shown not in _EDGE_SEEN:
+            raise FaceletError(f"edge at {EDGE_NAMES[pos]} has impossible colours {shown}")
+        edges.append(_EDGE_SEEN[shown])
 
-    if sorted(cp) != list(range(8)):
-        raise FaceletError("some corner appears twice")
-    if sorted(ep) != list(range(12)):
-        raise FaceletError("some edge appears twice")
-    if sum(co) % 3:
-        raise FaceletError("a corner is twisted (corner orientations do not sum to 0 mod 3)")
-    if sum(eo) % 2:
-        raise FaceletError("an edge is flipped (edge orientations do not sum to 0 mod 2)")
-    if permutation_parity(cp) != permutation_parity(ep):
-        raise FaceletError("two pieces are swapped (corner and edge permutation parities differ)")
+    cp, co = (list(x) for x in zip(*corners))
+    ep, eo = (list(x) for x in zip(*edges))
+    checks = ((len(set(cp)) == 8, "some corner appears twice"), (len(set(ep)) == 12, "some edge appears twice"),
+              (sum(co) % 3 == 0, "a corner is twisted (corner orientations do not sum to 0 mod 3)"),
+              (sum(eo) % 2 == 0, "an edge is flipped (edge orientations do not sum to 0 mod 2)"),
+              (permutation_parity(cp) == permutation_parity(ep),
+               "two pieces are swapped (corner and edge permutation parities differ)"))
+    for ok, message in checks:
+        if not ok:
+            raise FaceletError(message)
     return CubieState(tuple(cp), tuple(co), tuple(ep), tuple(eo))
 
 
