@@ -160,7 +160,11 @@ def config_table(args) -> str:
 
 
 def workload_config(args, world: int) -> dict:
-    n_hard = int(round(0.05 * args.batch))
+    n_hard = int(round(args.hard_frac * args.batch))
+    if n_hard == 0:
+        return {"workload": f"{args.batch} uniform random cubes (seed {args.seed}), {config_table(args)} table "
+                            "resident in HBM, one batch per step per GPU", "table": config_table(args),
+                "batch": args.batch, "hard": 0, "parallelism": f"replicas{world}"}
     return {"workload": f"batched: {args.batch} uniform random cubes (seed {args.seed}) with {n_hard} (5%) replaced by "
                         f"hard positions ({n_hard - 1} seed-20 uniform cubes of optimal length >= 19 and the superflip), "
                         f"{config_table(args)} table resident in HBM, one batch per step per GPU",
@@ -283,7 +287,7 @@ def reference_arm(args, world: int, rank: int, local: int) -> None:
         return
     from cuda_cube_solver import workloads
 
-    cubes, _ = workloads.batched_mix(args.batch, args.seed)
+    cubes, _ = workloads.batched_mix(args.batch, args.seed, args.hard_frac)
     table, _ = reference_table(args.kind, args.format, local)
     if args.warmup:  # a short warm-up window (page cache, thread start)
         cpu_window(args.kind, args.format, table, cubes[:64], min(2.0, args.cpu_step_s))
@@ -399,11 +403,11 @@ def main_arm(args, world: int, rank: int, local: int) -> None:
     build_passes = h.last_build_passes()
     solver.use_autotune = False
     solver.variant = args.variant
-    cubes, known = workloads.batched_mix(args.batch, rank_seed(args.seed, rank))
+    cubes, known = workloads.batched_mix(args.batch, rank_seed(args.seed, rank), args.hard_frac)
     tuned = None
     if args.tune:  # its own cubes: uniform ones of seed + 1000 and hard ones past those of the batch
         info = workloads.hard20()
-        n_hard = int(round(0.05 * args.batch)) - 1
+        n_hard = max(0, int(round(args.hard_frac * args.batch)) - 1)
         extra = workloads.uniform_cubes(info["indices"][-1] + 1, seed=20)
         sample = workloads.uniform_cubes(args.tune_cubes, seed=args.seed + 1000) + \
             [extra[i] for i in info["indices"][n_hard:n_hard + args.tune_hard]]
@@ -557,7 +561,8 @@ def main() -> None:
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--batch", type=int, default=4096, help="cubes per step and rank (5%% of them hard)")
+    ap.add_argument("--batch", type=int, default=4096, help="cubes per step and rank")
+    ap.add_argument("--hard-frac", type=float, default=0.05, help="share of the batch replaced by hard positions")
     ap.add_argument("--kind", default="d4t")
     ap.add_argument("--format", default="block", choices=["block", "b3"])
     ap.add_argument("--seed", type=int, default=2)

@@ -77,7 +77,9 @@ def batched_mix(n: int = 4096, seed: int = 2, hard_frac: float = 0.05) -> tuple[
     {position: known optimal length} of the hard ones."""
 
     cubes = uniform_cubes(n, seed=seed)
-    n_hard = max(1, int(round(hard_frac * n)))
+    n_hard = int(round(hard_frac * n))
+    if n_hard == 0:
+        return cubes, {}
     info = hard20()
     if n_hard - 1 > len(info["indices"]):
         raise ValueError(f"{n_hard - 1} hard cubes asked for; data/hard20.json lists {len(info['indices'])}")
