@@ -24,8 +24,12 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
     FramesSmem<THREADS> f;
     f.init(frame_smem, threadIdx.x);
 
+    // Per level of the lane's path: the move taken, the node's bounds, and the children not yet
+    // picked when it was left (a pop resumes exactly those: with LOOKAHEAD a sibling evaluated
+    // ahead of a pushed child, pruned or stashed, is not picked again, and a donation empties the
+    // entry of the level it gives away).
     unsigned char path[MAX_DEPTH];
-    uint32_t hstack[MAX_DEPTH];
+    uint32_t hstack[MAX_DEPTH], tstack[MAX_DEPTH];
     uint32_t h = 0, c = 0, todo = 0, ord = 0, rem = 0;
     uint32_t slot = 0, idx = 0, plen = 0, bound = 0, epoch = 0, pseq = 0;
     int g = 0, m = -1, k = 0;
@@ -36,12 +40,10 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
     const uint32_t lane_seed = (blockIdx.x * blockDim.x + threadIdx.x) * 0x9E3779B1u >> 7;
 
     // Work stealing: gbase = depth of the lane's unit root (0 for an item, the donated node's depth
-    // for a donated subtree); bit l of `cut` = the remaining children of the node at depth l were
-    // donated.  With LOOKAHEAD a sibling stashed at depth l stays with the donor (it resumes there
-    // when the subtree pops back) and is left out of the donation.
-    constexpr bool STEAL = true;
+    // for a donated subtree).  With LOOKAHEAD a sibling stashed at a donated depth stays with the
+    // donor (it was picked already, so it is not among the donated children).
     int gbase = 0;
-    uint32_t cut = 0, don_tick = 0;
+    uint32_t don_tick = 0;
     int mv = 0;  // frame update this lane waits for: 0 none, 1 push child m, 2 pop one level
     // LOOKAHEAD: the next sibling of the child under evaluation, evaluated alongside it; when the
     // child is pushed, the sibling's partial evaluation waits in a per-level stash (bit g of
@@ -109,6 +111,7 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                         }
                         m2 = -1;
                         hstack[g] = h;
+                        tstack[g] = todo;
                         path[g] = (unsigned char)m;
                         h = c;
                         ++g;
@@ -119,20 +122,8 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                     } else {
                         --g;
                         h = hstack[g];
-                        todo = 0u;
-                        if ((uint32_t)g >= plen) {
-                            int last = g > 0 ? path[g - 1] : -1;
-                            todo = T.amask[last + 1] & ~axis_move_mask(excluded_axes(h, bound - (uint32_t)g)) &
-                                   ~((2u << mm) - 1u);
-                            ord = frame_order(h, bound - (uint32_t)g);
-                        }
-                        if (STEAL) {
-                            cut &= (2u << g) - 1u;  // nodes below this one are gone: their marks too
-                            if ((cut >> g) & 1u) {  // this node's remaining children were donated
-                                todo = 0u;
-                                cut &= ~(1u << g);
-                            }
-                        }
+                        todo = tstack[g];
+                        if (todo) ord = frame_order(h, bound - (uint32_t)g);
                         if (LOOKAHEAD && ((stash >> g) & 1u)) {  // the stashed sibling resumes
                             stash &= ~(1u << g);
                             const uint32_t x = la_x[g];
@@ -140,7 +131,6 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                             rem = x & 0x3FFFFu;
                             m = (int)((x >> 18) & 31u);
                             k = (int)((x >> 23) & 7u);
-                            todo &= ~((2u << m) - 1u);
                         }
                     }
                     mv = 0;
@@ -164,7 +154,6 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
             atomicAdd(&sl.iter_nodes[bound < 24u ? bound : 23u], (unsigned long long)nodes);
             atomicAdd(&P.q->probes, (unsigned long long)probes);
             gbase = 0;
-            cut = 0u;
             if (finish_unit(P, slot)) {
                 if (*(volatile uint32_t*)&sl.found) {
                     finish_slot(P, slot, SLOT_SOLVED);
@@ -186,13 +175,9 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
             int r = fetch_item(P, seed, slot, idx, plen, bound, epoch);
             unsigned long long w1 = 0, w2 = 0, w3 = 0;
             bool donated_unit = false;
-            if (STEAL && r == FETCH_EMPTY && P.don_cap) {
+            if (r == FETCH_EMPTY && P.don_cap) {
                 donated_unit = take_donation(P, seed, slot, w1, w2, w3);
-                if (donated_unit) {
-                    r = FETCH_OK;
-                } else if (!*(volatile uint32_t*)&P.q->starving) {
-                    *(volatile uint32_t*)&P.q->starving = 1u;  // no item, no subtree: ask for donations
-                }
+                if (donated_unit) r = FETCH_OK;
             }
             if (r == FETCH_EMPTY) fetch_wait = 16;
             if (r == FETCH_FINISHED) {
@@ -203,11 +188,11 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                 Slot& sl = P.slots[slot];
                 if (*(volatile uint32_t*)&sl.found) {  // solved by another unit: count it done
                     if (finish_unit(P, slot)) finish_slot(P, slot, SLOT_SOLVED);
-                } else if (STEAL && donated_unit && (((w1 >> 32) & 31u) >= (uint32_t)MAX_DEPTH ||
+                } else if (donated_unit && (((w1 >> 32) & 31u) >= (uint32_t)MAX_DEPTH ||
                                                       ((w1 >> 37) & 31u) > MAX_BOUND)) {
                     atomicOr(&P.q->error, ERR_STACK);  // a malformed cell (never written by a donor)
                     if (finish_unit(P, slot)) finish_slot(P, slot, SLOT_ERROR);
-                } else if (STEAL && donated_unit) {
+                } else if (donated_unit) {
                     // a donated subtree: the node at depth g0 on the donor's path, its bounds and
                     // remaining children; the frames are the root's with the path replayed
                     const int g0 = (int)((w1 >> 32) & 31u);
@@ -226,7 +211,6 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                     pseq = 0;
                     nodes = 0;
                     probes = 0;
-                    cut = 0u;
                     stash = 0u;
                     m2 = -1;
                     todo = (uint32_t)(w1 >> 42) & 0x3FFFFu;
@@ -251,7 +235,7 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
         }
         // DONATE: while lanes starve, hand the remaining children of the shallowest node on this
         // lane's path that still has some (and enough depth left to be worth a replay) to them.
-        if (STEAL && P.don_cap && have && mv == 0 && (++don_tick & (P.don_period - 1u)) == 0u &&
+        if (P.don_cap && have && mv == 0 && (++don_tick & (P.don_period - 1u)) == 0u &&
             *(volatile uint32_t*)&P.q->starving) {
             volatile QueueState* q = P.q;
             if ((int)q->don_count >= (int)P.don_target) {
@@ -260,19 +244,9 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                 const int lo = gbase > (int)plen ? gbase : (int)plen;
                 for (int l = lo; l <= g; ++l) {
                     if (bound < (uint32_t)l + P.don_min_depth) break;
-                    uint32_t rest, hl;
-                    if (l == g) {
-                        rest = todo;
-                        hl = h;
-                    } else {
-                        if ((cut >> l) & 1u) continue;
-                        hl = hstack[l];
-                        const int last = l > 0 ? path[l - 1] : -1;
-                        rest = T.amask[last + 1] & ~axis_move_mask(excluded_axes(hl, bound - (uint32_t)l)) &
-                               ~((2u << path[l]) - 1u);
-                        if (LOOKAHEAD && ((stash >> l) & 1u)) rest &= ~(1u << ((la_x[l] >> 18) & 31u));
-                    }
+                    const uint32_t rest = l == g ? todo : tstack[l];
                     if (!rest) continue;
+                    const uint32_t hl = l == g ? h : hstack[l];
                     unsigned long long w2 = 0, w3 = 0;
                     for (int j = 0; j < l; ++j) {
                         if (j < 12) w2 |= (unsigned long long)path[j] << (5 * j);
@@ -282,10 +256,8 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                                                   ((unsigned long long)bound << 37) | ((unsigned long long)rest << 42);
                     atomicAdd(&P.slots[slot].open, 1u);  // before the post: the count never runs short
                     if (post_donation(P, lane_seed + don_tick, slot, w1, w2, w3)) {
-                        // the donated children are skipped here: now, and when a pop returns to
-                        // this node (a pop recomputes a node's remaining children from its path)
-                        if (l == g) todo = 0u;
-                        cut |= 1u << l;
+                        if (l == g) todo = 0u;  // the donated children are no longer this lane's
+                        else tstack[l] = 0u;
                     } else {
                         atomicSub(&P.slots[slot].open, 1u);  // (this lane's own unit keeps it above 0)
                     }
@@ -306,7 +278,11 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
         if (__all_sync(0xFFFFFFFFu, done)) break;
         const bool eval = mv == 0 && m >= 0 && k < 6;
         if (__ballot_sync(0xFFFFFFFFu, eval || have) == 0u) {
-            // Nothing queued for this warp: back off; leave after too many empty polls in a row.
+            // Nothing queued for this warp: ask lanes with work to donate subtrees (a whole idle
+            // warp, not a lane between two items, is the signal), back off, and leave after too
+            // many empty polls in a row.
+            if (lane == 0 && P.don_cap && !*(volatile uint32_t*)&P.q->starving)
+                *(volatile uint32_t*)&P.q->starving = 1u;
             if (++idle_polls > P.idle_limit) {
                 // A batch launch leaves (the host relaunches while cubes remain); a server launch
                 // leaves only when no cube is in flight, so every warp stays to serve new work.
