@@ -97,7 +97,8 @@ struct SearchParams {
     DonationCell* don;               // donation cells (null: no work stealing)
     uint32_t don_cap;                // number of cells
     uint32_t don_target;             // donors stop once this many subtrees wait
-    uint32_t don_min_depth;          // a donated node has at least this many moves left to the bound
+    uint32_t don_min_depth;          // a donated node has at least this many moves to the bound beyond
+                                     // its largest frame bound (its slack)
     uint32_t don_period;             // a lane with work checks for starving lanes every this many iterations
     uint32_t persistent;             // server: an empty queue is not the end (lanes wait for new cubes)
     unsigned long long* done_log;    // host-mapped completion log (server), may be null

@@ -247,6 +247,12 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
                     const uint32_t rest = l == g ? todo : tstack[l];
                     if (!rest) continue;
                     const uint32_t hl = l == g ? h : hstack[l];
+                    // slack: moves to the bound beyond the node's largest frame bound; a subtree
+                    // grows about 13x per move of slack, so a tight node is not worth a replay
+                    uint32_t hmax = 0;
+#pragma unroll
+                    for (int j = 0; j < 6; ++j) hmax = max(hmax, hget(hl, j));
+                    if (bound < (uint32_t)l + hmax + P.don_min_depth) continue;
                     unsigned long long w2 = 0, w3 = 0;
                     for (int j = 0; j < l; ++j) {
                         if (j < 12) w2 |= (unsigned long long)path[j] << (5 * j);

@@ -81,7 +81,7 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
     P->don = steal ? h->d_don : nullptr;
     P->don_cap = steal ? DON_CELLS : 0u;
     P->don_target = DON_CELLS / 8;
-    P->don_min_depth = o && o->steal_depth > 0 ? (uint32_t)o->steal_depth : 6u;
+    P->don_min_depth = o && o->steal_depth > 0 ? (uint32_t)o->steal_depth : 3u;
     P->don_period = 64;  // a power of two
     P->done_log = nullptr;
     P->done_log_cap = 0;

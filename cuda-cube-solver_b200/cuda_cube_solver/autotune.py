@@ -9,7 +9,8 @@ Knobs (``native.SolveOpts``):
 * ``base_plen``: cut depth of the work items (prefix length of a cube's iterations), 3-6;
 * ``move`` = (``move_min``, ``move_age``): how many lanes wait, and for how many iterations,
   before the frame-update pass (push / pop) runs -- the depth of the lanes' update pipeline, 1-16;
-* ``steal_depth``: the smallest subtree (moves left to the bound) a lane donates to idle lanes;
+* ``steal_depth``: the least slack (moves to the bound beyond a node's largest frame bound) of a
+  node whose children a lane donates to idle lanes;
 * ``spread``: over how many queued cubes the lanes spread;
 * ``probe_min``: a warp keeps probing while at least this many lanes have a probe.
 
@@ -34,11 +35,11 @@ SPACE = {
     "variant": [1, 2, 3, 6, 7],
     "base_plen": [3, 4, 5, 6],
     "move": [(1, 1), (4, 2), (8, 4), (16, 8)],
-    "steal_depth": [4, 6, 8],
+    "steal_depth": [2, 3, 4, 5],
     "spread": [512, 1024, 4096],
     "probe_min": [12, 16, 20, 24],
 }
-DEFAULT = {"variant": 1, "base_plen": 4, "move": (8, 4), "steal_depth": 6, "spread": 4096, "probe_min": 16}
+DEFAULT = {"variant": 1, "base_plen": 4, "move": (8, 4), "steal_depth": 3, "spread": 4096, "probe_min": 16}
 
 
 def opts_of(cfg: dict, timeout_s: float = 600.0) -> native.SolveOpts:

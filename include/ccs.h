@@ -144,7 +144,8 @@ typedef struct ccs_solve_opts {
                               /*   at least this many lanes have a probe (0: default, > 32: off) */
     int steal;                /* work stealing: lanes donate unexplored subtrees to idle lanes  */
                               /*   (phase-ordered variants 1-3, 6, 7; 0: on, < 0: off)          */
-    int steal_depth;          /* a donated subtree has at least this many moves to the bound (0: 6) */
+    int steal_depth;          /* a donated node's slack -- moves to the bound beyond its largest */
+                              /*   frame bound -- is at least this (0: 3)                       */
 } ccs_solve_opts;
 
 typedef struct ccs_result {

@@ -111,7 +111,7 @@ def test_work_stealing_keeps_lengths_and_iteration_nodes(lengths_golden, variant
     base = dict(timeout_s=900, variant=variant, deeper_at=(1e18, 1e18))
     off = h.solve(words, native.solve_opts(steal=-1, **base))
     assert h.last_solve_donations() == 0
-    for depth in (6, 3):
+    for depth in (3, 1):  # (slack 1: donations of small subtrees too, many of them)
         on = h.solve(words, native.solve_opts(steal=0, steal_depth=depth, **base))
         assert h.last_solve_donations() > 0
         _check_solutions(states, on)

@@ -13,7 +13,7 @@ from cuda_cube_solver import autotune, serving, workloads
 class FakeHandle:
     """Device time of a solve as a function of the settings, smallest at BEST."""
 
-    BEST = {"variant": 2, "base_plen": 5, "move": (4, 2), "steal_depth": 4, "spread": 1024, "probe_min": 12}
+    BEST = {"variant": 2, "base_plen": 5, "move": (4, 2), "steal_depth": 2, "spread": 1024, "probe_min": 12}
 
     def __init__(self):
         self.calls = []
