@@ -54,6 +54,7 @@ struct QueueState {
     unsigned long long donated;      // subtrees donated (diagnostic)
     uint32_t don_count;              // donated subtrees waiting in the donation cells
     uint32_t pad;
+    unsigned long long scan_pos;     // rotating start of the stranded-cube check
 };
 
 // A donated subtree: the unexplored children of one node of a running item (the node at depth g0

@@ -248,9 +248,13 @@ static __device__ __noinline__ void advance_head(const SearchParams& P) {
 }
 
 // Safety net run by an idle warp: queues any active cube whose current iteration still has items
-// to hand out but which has no ring entry (none should exist; the check is cheap).
+// to hand out but which has no ring entry (none should exist).  Each call checks the next 256
+// slots of a shared rotating window, so the check stays cheap however many slots there are.
 static __device__ __noinline__ void requeue_stranded(const SearchParams& P) {
-    for (uint32_t s = 0; s < P.n_slots; ++s) {
+    const uint32_t n = P.n_slots < 256u ? P.n_slots : 256u;
+    const uint32_t first = (uint32_t)(atomicAdd(&P.q->scan_pos, (unsigned long long)n) % P.n_slots);
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t s = (first + i) % P.n_slots;
         const Slot& sl = P.slots[s];
         if (*(const volatile uint32_t*)&sl.status != SLOT_ACTIVE || *(const volatile uint32_t*)&sl.found ||
             *(const volatile uint32_t*)&sl.queued)
