@@ -92,17 +92,18 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
 // 2 = the same with sibling lookahead (two probe chains per lane: lower latency when few cubes
 // are searched, more probes); 3 = phase-ordered, 256 x 3 (80 registers); 4 = loop control,
 // frames in registers, 256 x 2; 5 = loop control, frames in shared memory, 512 x 2;
-// 6 = phase-ordered, 128 x 4 (4 warps per block); 7 = phase-ordered, 512 x 1 (16 warps per block).
+// 6 = phase-ordered, 128 x 4 (4 warps per block); 7 = phase-ordered, 512 x 1 (16 warps per block);
+// 8 = sibling lookahead, 256 x 3.
 // 0 = automatic: 2 for fewer than 64 cubes (and for the server), else 1.
 int resolve_variant(const ccs_solve_opts* o, int cubes) {
     int v = o ? o->variant : 0;
-    if (v <= 0 || v > 7) v = cubes < 64 ? 2 : 1;
+    if (v <= 0 || v > 8) v = cubes < 64 ? 2 : 1;
     return v;
 }
 
 int grid_for(ccs_handle* h, const ccs_solve_opts* o, int variant) {
     int bps = o && o->blocks_per_sm > 0 ? o->blocks_per_sm
-                                         : (variant == 3 ? 3 : variant == 6 ? 4 : variant == 7 ? 1 : 2);
+                                         : (variant == 3 || variant == 8 ? 3 : variant == 6 ? 4 : variant == 7 ? 1 : 2);
     return bps * h->sms;
 }
 
