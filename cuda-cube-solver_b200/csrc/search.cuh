@@ -101,6 +101,7 @@ struct SearchParams {
     uint32_t don_min_depth;          // a donated node has at least this many moves to the bound beyond
                                      // its largest frame bound (its slack)
     uint32_t don_period;             // a lane with work checks for starving lanes every this many iterations
+    uint32_t don_eager;              // 1: a lane without work asks for donations (0: a whole idle warp)
     uint32_t persistent;             // server: an empty queue is not the end (lanes wait for new cubes)
     unsigned long long* done_log;    // host-mapped completion log (server), may be null
     uint32_t done_log_cap;

@@ -178,6 +178,8 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
             if (r == FETCH_EMPTY && P.don_cap) {
                 donated_unit = take_donation(P, seed, slot, w1, w2, w3);
                 if (donated_unit) r = FETCH_OK;
+                else if (P.don_eager && !*(volatile uint32_t*)&P.q->starving)
+                    *(volatile uint32_t*)&P.q->starving = 1u;  // eager: any lane without work asks
             }
             if (r == FETCH_EMPTY) fetch_wait = 16;
             if (r == FETCH_FINISHED) {

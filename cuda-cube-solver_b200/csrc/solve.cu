@@ -80,9 +80,12 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
     const bool steal = h->d_don && !(o && o->steal < 0);
     P->don = steal ? h->d_don : nullptr;
     P->don_cap = steal ? DON_CELLS : 0u;
-    P->don_target = DON_CELLS / 8;
+    P->don_target = o && o->steal_target > 0 ? (uint32_t)std::min<int>(o->steal_target, (int)DON_CELLS) : DON_CELLS / 8;
     P->don_min_depth = o && o->steal_depth > 0 ? (uint32_t)o->steal_depth : 3u;
-    P->don_period = 64;  // a power of two
+    uint32_t period = o && o->steal_period > 0 ? (uint32_t)o->steal_period : 64u;
+    while (period & (period - 1)) period &= period - 1;  // a power of two (rounded down)
+    P->don_period = period;
+    P->don_eager = o && o->steal > 0 ? 1u : 0u;
     P->done_log = nullptr;
     P->done_log_cap = 0;
 }

@@ -143,9 +143,13 @@ typedef struct ccs_solve_opts {
     int probe_min;            /* a warp keeps probing (pruned children -> next sibling) while  */
                               /*   at least this many lanes have a probe (0: default, > 32: off) */
     int steal;                /* work stealing: lanes donate unexplored subtrees to idle lanes  */
-                              /*   (phase-ordered variants 1-3, 6, 7; 0: on, < 0: off)          */
+                              /*   (phase-ordered variants 1-3, 6-8; 0: on, asked for by idle   */
+                              /*   warps; 1: on, asked for by any idle lane; < 0: off)          */
     int steal_depth;          /* a donated node's slack -- moves to the bound beyond its largest */
                               /*   frame bound -- is at least this (0: 3)                       */
+    int steal_period;         /* a lane with work checks for starving lanes every this many    */
+                              /*   iterations, a power of two (0: 64)                           */
+    int steal_target;         /* donors stop once this many subtrees wait (0: 512)              */
 } ccs_solve_opts;
 
 typedef struct ccs_result {
