@@ -39,7 +39,7 @@ struct Server {
     bool kernel_running = false;
     SearchParams P{};
     int grid = 0;
-    int variant = 2;  // resolved kernel variant (automatic: sibling lookahead, for latency)
+    int variant = 3;  // resolved kernel variant
     unsigned long long* done_log = nullptr;  // host-mapped
     unsigned long long* d_done_log = nullptr;
     uint32_t log_cap = 0;

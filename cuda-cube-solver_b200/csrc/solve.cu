@@ -81,11 +81,14 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
     P->don = steal ? h->d_don : nullptr;
     P->don_cap = steal ? DON_CELLS : 0u;
     P->don_target = o && o->steal_target > 0 ? (uint32_t)std::min<int>(o->steal_target, (int)DON_CELLS) : DON_CELLS / 8;
-    P->don_min_depth = o && o->steal_depth > 0 ? (uint32_t)o->steal_depth : 3u;
+    P->don_min_depth = o && o->steal_depth > 0 ? (uint32_t)o->steal_depth : 2u;
     uint32_t period = o && o->steal_period > 0 ? (uint32_t)o->steal_period : 64u;
     while (period & (period - 1)) period &= period - 1;  // a power of two (rounded down)
     P->don_period = period;
-    P->don_eager = o && o->steal > 0 ? 1u : 0u;
+    // Any lane without work asks for donations (steal 0), or only whole idle warps (steal 2).
+    // Measured on B200 with 256 x 3: the 4,096-cube batch with 5% hard positions 220 against 194
+    // cubes/s, a lone superflip on d4t 3.1 against 5.8 s, uniform batches within 4%.
+    P->don_eager = o && o->steal == 2 ? 0u : 1u;
     P->done_log = nullptr;
     P->done_log_cap = 0;
 }
@@ -97,10 +100,13 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
 // frames in registers, 256 x 2; 5 = loop control, frames in shared memory, 512 x 2;
 // 6 = phase-ordered, 128 x 4 (4 warps per block); 7 = phase-ordered, 512 x 1 (16 warps per block);
 // 8 = sibling lookahead, 256 x 3.
-// 0 = automatic: 2 for fewer than 64 cubes (and for the server), else 1.
+// 0 = automatic: 2 for fewer than 64 cubes, else 3 (and 3 for the server).  Measured on B200
+// (d4t, 1,024 uniform cubes): 3 reaches 338 cubes/s (31.0 G probes/s) against 283 for 1 and 292
+// for 2 -- its 80-register cap spills a little, to an L1 that the table sectors no longer
+// occupy; a lone cube is faster on 2 (plain 1-cube p50 16.6 ms against 25.0 ms).
 int resolve_variant(const ccs_solve_opts* o, int cubes) {
     int v = o ? o->variant : 0;
-    if (v <= 0 || v > 8) v = cubes < 64 ? 2 : 1;
+    if (v <= 0 || v > 8) v = cubes > 0 && cubes < 64 ? 2 : 3;
     return v;
 }
 

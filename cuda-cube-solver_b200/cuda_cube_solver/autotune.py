@@ -32,14 +32,14 @@ from cuda_cube_solver.device import state_words
 CACHE = Path(os.environ.get("CCS_TUNE_CACHE", Path.home() / ".cache" / "cuda_cube_solver" / "autotune.json"))
 
 SPACE = {
-    "variant": [1, 2, 3, 6, 7],
+    "variant": [3, 1, 2, 8, 6, 7],
     "base_plen": [3, 4, 5, 6],
     "move": [(1, 1), (4, 2), (8, 4), (16, 8)],
-    "steal_depth": [2, 3, 4, 5],
+    "steal_depth": [1, 2, 3, 4],
     "spread": [512, 1024, 4096],
     "probe_min": [12, 16, 20, 24],
 }
-DEFAULT = {"variant": 1, "base_plen": 4, "move": (8, 4), "steal_depth": 3, "spread": 4096, "probe_min": 16}
+DEFAULT = {"variant": 3, "base_plen": 4, "move": (8, 4), "steal_depth": 2, "spread": 4096, "probe_min": 16}
 
 
 def opts_of(cfg: dict, timeout_s: float = 600.0) -> native.SolveOpts:

@@ -133,9 +133,10 @@ typedef struct ccs_solve_opts {
     int threads;              /* threads per block: 128, 256 or 512 (0: default)            */
     double timeout_s;         /* give up after this long (0: no limit)                      */
     int spread;               /* lanes work on up to this many queued cubes at once (0: 4096) */
-    int variant;              /* search kernel: 0 automatic, 1 throughput, 2 sibling lookahead */
-                              /*   (latency), 3-7 other launch shapes: 3 = 256 x 3 blocks/SM,  */
-                              /*   6 = 128 x 4, 7 = 512 x 1 (4-5: loop-control forms)           */
+    int variant;              /* search kernel: 0 automatic (2 below 64 cubes, else 3), 1 = 256 */
+                              /*   threads x 2 blocks/SM, 2 = sibling lookahead (two probe      */
+                              /*   chains per lane), 3 = 256 x 3, 6 = 128 x 4, 7 = 512 x 1,      */
+                              /*   8 = lookahead 256 x 3 (4-5: loop-control forms)              */
     double shallow_at0;       /* an iteration of < this many nodes makes the next one use a    */
     double shallow_at1;       /*   prefix one move shorter (0: 1e5 / 1.5e6, < 0: off)          */
     int move_min;             /* lanes waiting before a frame-update pass runs (0: 8)          */
@@ -143,10 +144,10 @@ typedef struct ccs_solve_opts {
     int probe_min;            /* a warp keeps probing (pruned children -> next sibling) while  */
                               /*   at least this many lanes have a probe (0: default, > 32: off) */
     int steal;                /* work stealing: lanes donate unexplored subtrees to idle lanes  */
-                              /*   (phase-ordered variants 1-3, 6-8; 0: on, asked for by idle   */
-                              /*   warps; 1: on, asked for by any idle lane; < 0: off)          */
+                              /*   (phase-ordered variants 1-3, 6-8; 0 or 1: on, asked for by   */
+                              /*   any idle lane; 2: on, asked for by whole idle warps; < 0: off) */
     int steal_depth;          /* a donated node's slack -- moves to the bound beyond its largest */
-                              /*   frame bound -- is at least this (0: 3)                       */
+                              /*   frame bound -- is at least this (0: 2)                       */
     int steal_period;         /* a lane with work checks for starving lanes every this many    */
                               /*   iterations, a power of two (0: 64)                           */
     int steal_target;         /* donors stop once this many subtrees wait (0: 512)              */
