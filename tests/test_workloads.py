@@ -45,3 +45,40 @@ def test_flipped_edges_and_the_table_rule():
     assert n[0] == 0 and n[1] == 12
     assert all(x % 2 == 0 for x in n)  # edge flips have even parity
     assert (n >= FLIP_RULE).sum() >= 1 and FLIP_RULE == 12
+
+
+def test_batched_mix_workload():
+    """The batched configuration: 4,096 uniform cubes of seed 2 with 205 (5%) replaced by hard
+    positions -- 204 seed-20 cubes of known optimal length >= 19 (lengths confirmed by the
+    reference's kernels when the fixture was made) and the superflip."""
+
+    from cuda_cube_solver import workloads
+
+    info = workloads.hard20()
+    assert info["reference_equal"] and len(info["indices"]) >= 204
+    assert all(L >= 19 for L in info["lengths"])
+    cubes, known = workloads.batched_mix(4096, seed=2)
+    assert len(cubes) == 4096 and len(known) == 205
+    assert all(c.is_legal() for c in cubes)
+    assert sorted(known.values()).count(20) >= 1 and min(known.values()) >= 19
+    assert workloads.superflip() in [cubes[i] for i in known]
+    again, known2 = workloads.batched_mix(4096, seed=2)
+    assert again == cubes and known2 == known
+    uniform, none = workloads.batched_mix(64, seed=2, hard_frac=0.0)
+    assert none == {} and uniform == workloads.uniform_cubes(64, seed=2)
+
+
+def test_bfs_roofline_arithmetic():
+    import sys
+
+    from conftest import ROOT
+
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    passes = [{"depth": 1, "forward": True, "found": 2, "random_reads": 10, "claims": 6, "seconds": 0.5},
+              {"depth": 2, "forward": False, "found": 5, "random_reads": 100, "claims": 0, "seconds": 1.5}]
+    r = bench.bfs_roofline(passes, entries=1000, peak_gbs=1.0, ceiling=50.0)
+    assert r["dominant_pass"] == {"depth": 2, "dir": "bwd", "seconds": 1.5} and r["dominant_share"] == 0.75
+    assert r["passes"][0]["algorithmic_gb"] == (1000 + 32 * 16) / 1e9
+    assert abs(r["frac_of_random_sector_ceiling"] - (100 / 1.5) / 50.0) < 1e-12
