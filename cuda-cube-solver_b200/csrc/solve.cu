@@ -69,7 +69,7 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
     P->shallow_min_active = 32;
     // A lone 20-move cube on B200: deeper prefixes from 1e6 / 6e7 nodes instead of 5e7 / 3e9 took
     // the superflip from 1.66 to 0.74 s on d4 and from 12.7 to 7.5 s on d4t.
-    P->few_divisor = 50;
+    P->few_divisor = o && o->few_divisor > 0 ? (uint32_t)o->few_divisor : 50u;
     P->few_max_active = 4;  // (the server sets 0: see ccs_server_start)
     P->idle_limit = 1u << 21;  // ~8 s of idle polling (4 us back-off) before a warp leaves
     P->spread = o && o->spread > 0 ? (uint32_t)o->spread : 4096u;

@@ -88,7 +88,7 @@ class GpuSolver:
                  inverse: bool = True, collect_stats: bool = False, mode: str = "step",
                  extra_tables: int = 2, step_extra: int = 0, table_format: str = "block",
                  step_defines: tuple[str, ...] = (), kind="d4t",
-                 deeper_prefix_at: tuple[float, ...] = (5e7, 3e9), extra_kind=None,
+                 deeper_prefix_at: tuple[float, ...] | None = None, extra_kind=None,
                  handle: native.Handle | None = None, device: int = 0):
         # The reference's keywords (solver.py:119-123) are all accepted; those of its experimental
         # search modes (extra tables, extra kinds, NVRTC defines) are not built and are refused
@@ -111,6 +111,11 @@ class GpuSolver:
         if table_format not in native.FORMATS:
             raise ValueError(f"unknown table format {table_format!r}")
         self.prefix_len = prefix_len
+        # Given explicitly, the thresholds mean what they mean in the reference (no few-cube
+        # division); by default the library also deepens prefixes sooner for a lone hard cube.
+        self.exact_thresholds = deeper_prefix_at is not None
+        if deeper_prefix_at is None:
+            deeper_prefix_at = (5e7, 3e9)
         self.deeper_prefix_at = tuple(deeper_prefix_at) + (float("inf"),) * (2 - len(deeper_prefix_at))
         self.collect_stats = collect_stats
         if handle is None:
@@ -168,7 +173,7 @@ class GpuSolver:
     def _opts(self, timeout_s: float = 0.0, n: int = 0) -> native.SolveOpts:
         blocks_per_sm = max(1, round(self.grid / self.sms)) if self.grid else 0
         o = native.solve_opts(self.prefix_len, self.deeper_prefix_at[:2], blocks_per_sm, 0, timeout_s,
-                              variant=self.variant)
+                              variant=self.variant, few_divisor=1 if self.exact_thresholds else 0)
         tuned = self.tuned if self.tuned is not None else None
         if tuned is None and self.use_autotune:
             from cuda_cube_solver import autotune

@@ -127,8 +127,8 @@ int ccs_root_bounds(ccs_handle* h, const uint32_t* states, int n, uint32_t* out_
 typedef struct ccs_solve_opts {
     int base_plen;            /* prefix length of a cube's first iterations (reference: 4) */
     double deeper_at0;        /* an iteration of >= this many nodes makes the next one use a */
-    double deeper_at1;        /*   prefix one move longer (reference: 5e7, 3e9); in ccs_solve */
-                              /*   both are divided by 50 while at most 4 cubes are in flight */
+    double deeper_at1;        /*   prefix one move longer (reference: 5e7, 3e9); see also     */
+                              /*   few_divisor                                                */
     int blocks_per_sm;        /* persistent grid = blocks_per_sm * SMs (0: default)         */
     int threads;              /* threads per block: 128, 256 or 512 (0: default)            */
     double timeout_s;         /* give up after this long (0: no limit)                      */
@@ -151,6 +151,8 @@ typedef struct ccs_solve_opts {
     int steal_period;         /* a lane with work checks for starving lanes every this many    */
                               /*   iterations, a power of two (0: 64)                           */
     int steal_target;         /* donors stop once this many subtrees wait (0: 512)              */
+    int few_divisor;          /* while at most 4 cubes are in flight, deeper_at0/1 are divided */
+                              /*   by this (0: 50; 1: never, the reference's plain thresholds)  */
 } ccs_solve_opts;
 
 typedef struct ccs_result {
