@@ -569,7 +569,7 @@ def main() -> None:
     ap.add_argument("--impl", default="mine", choices=["mine", "reference", "reference-gpu"])
     ap.add_argument("--variant", type=int, default=0, help="search kernel variant (ccs_solve_opts.variant)")
     ap.add_argument("--no-tune", dest="tune", action="store_false", help="skip the autotuner (library defaults)")
-    ap.add_argument("--tune-budget", type=float, default=90.0, help="seconds of autotuning at most")
+    ap.add_argument("--tune-budget", type=float, default=60.0, help="seconds of autotuning at most")
     ap.add_argument("--tune-cubes", type=int, default=512)
     ap.add_argument("--tune-hard", type=int, default=8)
     ap.add_argument("--plain", type=int, default=1000, help="cubes solved one per call (0: skip)")
