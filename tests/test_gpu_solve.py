@@ -142,3 +142,17 @@ def test_lone_superflip_with_stealing(lengths_golden):
     res = h.solve(words, native.solve_opts(timeout_s=900, variant=1))
     assert res[0].length == c["length"]
     assert h.last_solve_donations() > 0
+
+
+def test_autotuned_settings_give_the_same_lengths(lengths_golden):
+    """The autotuner's choice (a short descent on its own sample) changes speed only: the tuned
+    solver returns the reference's optimal lengths."""
+
+    h = resident_handle("d4t")
+    solver = GpuSolver(kind="d4t", handle=h)
+    sample = [_state(parse_moves(c["scramble"])) for c in lengths_golden["random1000"][700:764]]
+    result = solver.autotune(sample, save=False, budget_s=20.0)
+    assert result["trials"] >= 1 and solver.tuned == result["config"]
+    cubes = lengths_golden["random1000"][764:828]
+    sols = solver.solve([_state(parse_moves(c["scramble"])) for c in cubes])
+    assert [len(s.moves) for s in sols] == [c["length"] for c in cubes]
