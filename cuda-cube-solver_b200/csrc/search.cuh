@@ -102,6 +102,7 @@ struct SearchParams {
                                      // its largest frame bound (its slack)
     uint32_t don_period;             // a lane with work checks for starving lanes every this many iterations
     uint32_t don_eager;              // 1: a lane without work asks for donations (0: a whole idle warp)
+    unsigned long long don_min_prev; // donate for cubes whose previous iteration had >= this many nodes
     uint32_t persistent;             // server: an empty queue is not the end (lanes wait for new cubes)
     unsigned long long* done_log;    // host-mapped completion log (server), may be null
     uint32_t done_log_cap;

@@ -236,9 +236,12 @@ __global__ void __launch_bounds__(THREADS, MINB) search_kernel_phased(const DevT
             }
         }
         // DONATE: while lanes starve, hand the remaining children of the shallowest node on this
-        // lane's path that still has some (and enough depth left to be worth a replay) to them.
+        // lane's path that still has some (and enough slack to be worth a replay) to them -- for
+        // a cube whose previous iteration reached P.don_min_prev nodes (its current one is big).
         if (P.don_cap && have && mv == 0 && (++don_tick & (P.don_period - 1u)) == 0u &&
-            *(volatile uint32_t*)&P.q->starving) {
+            *(volatile uint32_t*)&P.q->starving &&
+            (P.don_min_prev == 0ull || (bound > 0u && *(volatile unsigned long long*)&P.slots[slot].iter_nodes[
+                                                         (bound - 1u) < 24u ? bound - 1u : 23u] >= P.don_min_prev))) {
             volatile QueueState* q = P.q;
             if ((int)q->don_count >= (int)P.don_target) {
                 q->starving = 0u;

@@ -89,6 +89,8 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
     // Measured on B200 with 256 x 3: the 4,096-cube batch with 5% hard positions 220 against 194
     // cubes/s, a lone superflip on d4t 3.1 against 5.8 s, uniform batches within 4%.
     P->don_eager = o && o->steal == 2 ? 0u : 1u;
+    P->don_min_prev = o && o->steal_min_nodes != 0 ? (o->steal_min_nodes > 0 ? (unsigned long long)o->steal_min_nodes : 0ull)
+                                                   : 10000000ull;
     P->done_log = nullptr;
     P->done_log_cap = 0;
 }

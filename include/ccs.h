@@ -153,6 +153,8 @@ typedef struct ccs_solve_opts {
     int steal_target;         /* donors stop once this many subtrees wait (0: 512)              */
     int few_divisor;          /* while at most 4 cubes are in flight, deeper_at0/1 are divided */
                               /*   by this (0: 50; 1: never, the reference's plain thresholds)  */
+    double steal_min_nodes;   /* subtrees of a cube are donated only once its previous          */
+                              /*   iteration reached this many nodes (0: 1e7; < 0: always)      */
 } ccs_solve_opts;
 
 typedef struct ccs_result {

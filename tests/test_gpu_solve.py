@@ -112,7 +112,7 @@ def test_work_stealing_keeps_lengths_and_iteration_nodes(lengths_golden, variant
     off = h.solve(words, native.solve_opts(steal=-1, **base))
     assert h.last_solve_donations() == 0
     for depth in (3, 1):  # (slack 1: donations of small subtrees too, many of them)
-        on = h.solve(words, native.solve_opts(steal=0, steal_depth=depth, **base))
+        on = h.solve(words, native.solve_opts(steal=0, steal_depth=depth, steal_min_nodes=-1, **base))
         assert h.last_solve_donations() > 0
         _check_solutions(states, on)
         assert [r.length for r in on] == [r.length for r in off] == [c["length"] for c in cubes]
