@@ -134,7 +134,7 @@ __device__ __forceinline__ uint32_t edge_coord_sym(const DevTables& T, const Sta
         uint32_t eord = T.cmp4[em0][labels8(p0)] | ((uint32_t)T.cmp4[em1][labels8(p1)] << (2 * n0)) |
                         ((uint32_t)T.cmp4[em2][labels8(p2)] << (2 * (n0 + n1)));
         const uint16_t* genc = second ? T.genc2 : T.genc;
-        return (slice * 256u + nflips) * (uint32_t)NEC + genc[((uint32_t)T.sy_lab[sym][eord] << 4) | eflips];
+        return (slice * 256u + nflips) * (uint32_t)NEC + genc[((uint32_t)T.sy_lab[sym][eord] << 4) | eflips];  // rank * 16 + flips
     }
 }
 

@@ -21,13 +21,8 @@ bool allowed_after(int last, int m) {
 }
 }  // namespace
 
-void build_genc(const KindDesc& kind, uint16_t genc[4096]) {
-    std::memset(genc, 0, 4096 * sizeof(uint16_t));
-    for (int e = 0; e < 256; ++e) {
-        uint8_t r = eorder_rank()[e];
-        if (r == 0xFF) continue;
-        for (int f = 0; f < 16; ++f) genc[(e << 4) | f] = kind.gen_class[r * 16 + f];
-    }
+void build_genc(const KindDesc& kind, uint16_t genc[384]) {
+    for (int c = 0; c < 384; ++c) genc[c] = kind.gen_class[c];
 }
 
 void build_dev_tables(const KindDesc& kind, DevTables* T) {
@@ -101,7 +96,8 @@ void build_dev_tables(const KindDesc& kind, DevTables* T) {
         for (int v = 0; v < 256; ++v) {
             uint32_t out = 0;
             for (int j = 0; j < 4; ++j) out |= (uint32_t)(a.eperm[8 + ((v >> (2 * j)) & 3)] - 8) << (2 * j);
-            T->sy_lab[s][v] = (uint8_t)out;
+            const uint8_t r = eorder_rank()[out];
+            T->sy_lab[s][v] = r == 0xFF ? 0 : r;  // (label strings that are no order never occur)
         }
     }
     for (int i = 0; i < 4096; ++i) T->slice_rank[i] = slice_rank()[i] == 0xFFFF ? 0 : slice_rank()[i];

@@ -28,15 +28,16 @@ struct alignas(16) DevTables {
     uint32_t sy_pflp[16][3];
     uint32_t sy_rel[16][3];
     // What the cubie relabel of a U-D symmetry does to the coordinate: E cubies stay E cubies
-    // (labels permuted by sy_lab, on a compacted 2-bit label string), U cubies all become U or all
-    // become D (sy_swap), and the flips of E positions and of E cubies toggle together (sy_fx).
+    // (labels permuted: sy_lab maps a compacted 2-bit label string to the rank of the relabelled
+    // order, 0..23), U cubies all become U or all become D (sy_swap), and the flips of E positions
+    // and of E cubies toggle together (sy_fx).
     uint8_t sy_lab[16][256];
     uint8_t sy_fx[16];
     uint8_t sy_swap[16];
     uint16_t slice_rank[4096];   // 12-bit E mask -> 0..494
     uint16_t slice_unrank[496];
-    uint16_t genc[4096];         // (E labels in position order, 8 bits) << 4 | E flips -> class
-    uint16_t genc2[4096];        // the same for a second resident table of a compatible kind
+    uint16_t genc[384];          // E content (order rank * 16 + E flips) -> class
+    uint16_t genc2[384];         // the same for a second resident table of a compatible kind
     uint16_t gen_rep[2][384];    // class -> content (order rank * 16 + flips), by flip parity
     uint8_t cmp4[16][256];       // 2-bit fields of a byte selected by a 4-bit mask, compacted
     uint8_t flp[256];            // (E mask4 << 4 | flip mask4) -> E flips | non-E flips << 4
@@ -57,7 +58,7 @@ struct alignas(16) DevTables {
 void build_dev_tables(const KindDesc& kind, DevTables* out);
 
 // The E-content class table of a kind, as genc / genc2 hold it.
-void build_genc(const KindDesc& kind, uint16_t genc[4096]);
+void build_genc(const KindDesc& kind, uint16_t genc[384]);
 
 }  // namespace ccs
 

@@ -157,7 +157,7 @@ static int attach_second(ccs_handle* h, const char* kind, int format, uint32_t* 
     CCS_TRY(get_kind(kind, &k2));
     if (!h->d_table || h->format != format || k2.mode != h->kind.mode || k2.nec != h->kind.nec)
         return fail(CCS_E_ARG, "a second table must match the first one's kind family and format");
-    uint16_t genc[4096];
+    uint16_t genc[384];
     build_genc(k2, genc);
     CCS_CUDA_TRY(cudaMemcpy(reinterpret_cast<char*>(h->d_tables) + offsetof(DevTables, genc2), genc, sizeof genc,
                             cudaMemcpyHostToDevice));
