@@ -29,7 +29,7 @@ int launch_phased(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t s
     return CCS_OK;
 }
 
-// Kernel variants (ccs_solve_opts.variant, resolved 1..9): see resolve_variant in solve.cu.
+// Kernel variants (ccs_solve_opts.variant, resolved 1..11): see resolve_variant in solve.cu.
 template <int MODE, int NEC>
 int launch_kind(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t stream, int variant) {
     return dispatch_fmt(h->format, [&](auto F) {
@@ -42,6 +42,8 @@ int launch_kind(ccs_handle* h, const SearchParams& P, int grid, cudaStream_t str
         if (variant == 7) return launch_phased<MODE, NEC, FMT, 512, 1>(h, P, grid, stream);
         if (variant == 8) return launch_phased<MODE, NEC, FMT, 256, 3, true>(h, P, grid, stream);
         if (variant == 9) return launch_phased<MODE, NEC, FMT, 256, 4>(h, P, grid, stream);
+        if (variant == 10) return launch_phased<MODE, NEC, FMT, 224, 3>(h, P, grid, stream);
+        if (variant == 11) return launch_phased<MODE, NEC, FMT, 128, 5>(h, P, grid, stream);
         return launch_phased<MODE, NEC, FMT, 256, 2>(h, P, grid, stream);
     });
 }
@@ -62,6 +64,8 @@ int kernel_footprint_kind(ccs_handle* h, int variant, size_t* local_bytes, int* 
         else if (variant == 7) e = (t = 512, cudaFuncGetAttributes(&a, search_kernel_phased<MODE, NEC, FMT, 512, 1>));
         else if (variant == 8) e = cudaFuncGetAttributes(&a, search_kernel_phased<MODE, NEC, FMT, 256, 3, true>);
         else if (variant == 9) e = cudaFuncGetAttributes(&a, search_kernel_phased<MODE, NEC, FMT, 256, 4>);
+        else if (variant == 10) e = (t = 224, cudaFuncGetAttributes(&a, search_kernel_phased<MODE, NEC, FMT, 224, 3>));
+        else if (variant == 11) e = (t = 128, cudaFuncGetAttributes(&a, search_kernel_phased<MODE, NEC, FMT, 128, 5>));
         else e = cudaFuncGetAttributes(&a, search_kernel_phased<MODE, NEC, FMT, 256, 2>);
         CCS_CUDA_TRY(e);
         *local_bytes = a.localSizeBytes;

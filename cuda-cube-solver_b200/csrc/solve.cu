@@ -101,20 +101,24 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
 // are searched, more probes); 3 = phase-ordered, 256 x 3 (80 registers); 4 = loop control,
 // frames in registers, 256 x 2; 5 = loop control, frames in shared memory, 512 x 2;
 // 6 = phase-ordered, 128 x 4 (4 warps per block); 7 = phase-ordered, 512 x 1 (16 warps per block);
-// 8 = sibling lookahead, 256 x 3; 9 = phase-ordered, 256 x 4 (32 warps per SM, 64 registers).
+// 8 = sibling lookahead, 256 x 3; 9 = phase-ordered, 256 x 4 (32 warps per SM, 64 registers);
+// 10 = phase-ordered, 224 x 3 (21 warps, 96 registers); 11 = phase-ordered, 128 x 5 (20 warps, 96).
 // 0 = automatic: 2 for fewer than 64 cubes, else 3 (and 3 for the server).  Measured on B200
 // (d4t, 1,024 uniform cubes): 3 reaches 338 cubes/s (31.0 G probes/s) against 283 for 1 and 292
 // for 2 -- its 80-register cap spills a little, to an L1 that the table sectors no longer
 // occupy; a lone cube is faster on 2 (plain 1-cube p50 16.6 ms against 25.0 ms).
 int resolve_variant(const ccs_solve_opts* o, int cubes) {
     int v = o ? o->variant : 0;
-    if (v <= 0 || v > 9) v = cubes > 0 && cubes < 64 ? 2 : 3;
+    if (v <= 0 || v > 11) v = cubes > 0 && cubes < 64 ? 2 : 3;
     return v;
 }
 
 int grid_for(ccs_handle* h, const ccs_solve_opts* o, int variant) {
     int bps = o && o->blocks_per_sm > 0 ? o->blocks_per_sm
-                                         : (variant == 3 || variant == 8 ? 3 : variant == 6 || variant == 9 ? 4 : variant == 7 ? 1 : 2);
+                                         : (variant == 3 || variant == 8 || variant == 10 ? 3
+                                          : variant == 6 || variant == 9 ? 4
+                                          : variant == 11 ? 5
+                                          : variant == 7 ? 1 : 2);
     return bps * h->sms;
 }
 

@@ -32,7 +32,7 @@ from cuda_cube_solver.device import state_words
 CACHE = Path(os.environ.get("CCS_TUNE_CACHE", Path.home() / ".cache" / "cuda_cube_solver" / "autotune.json"))
 
 SPACE = {
-    "variant": [3, 1, 2, 8, 6, 7],
+    "variant": [3, 1, 2, 8, 10, 11, 6, 7, 9],
     "base_plen": [3, 4, 5, 6],
     "move": [(1, 1), (4, 2), (8, 4), (16, 8)],
     "steal_depth": [1, 2, 3, 4],

@@ -126,7 +126,7 @@ def test_launch_shapes_agree(lengths_golden):
     h = resident_handle("d4t")
     cubes = lengths_golden["random1000"][300:364]
     words = state_words([_state(parse_moves(c["scramble"])) for c in cubes])
-    for variant in (1, 2, 3, 4, 5, 6, 7, 8, 9):
+    for variant in (1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11):
         res = h.solve(words, native.solve_opts(timeout_s=600, variant=variant))
         assert [r.length for r in res] == [c["length"] for c in cubes], variant
     h2d, d2h = h.last_solve_io_bytes()
