@@ -3,9 +3,10 @@ GPU, table and batch size by measuring them.
 
 Knobs (``native.SolveOpts``):
 
-* ``variant``: search kernel and launch shape -- 1 = 256 threads x 2 blocks per SM (the
-  throughput kernel), 2 = the same with sibling lookahead (two probe chains per lane), 3 = 256 x
-  3, 6 = 128 x 4 (4 warps per block), 7 = 512 x 1 (16 warps per block);
+* ``variant``: search kernel and launch shape -- 3 = 256 threads x 3 blocks per SM (the batched
+  default), 1 = 256 x 2, 2 = 256 x 2 with sibling lookahead (two probe chains per lane), 8 =
+  lookahead 256 x 3, 10 = 224 x 3, 11 = 128 x 5, 6 = 128 x 4 (4 warps per block), 7 = 512 x 1
+  (16 warps per block), 9 = 256 x 4 (32 warps per SM);
 * ``base_plen``: cut depth of the work items (prefix length of a cube's iterations), 3-6;
 * ``move`` = (``move_min``, ``move_age``): how many lanes wait, and for how many iterations,
   before the frame-update pass (push / pop) runs -- the depth of the lanes' update pipeline, 1-16;
