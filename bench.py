@@ -411,7 +411,7 @@ def main_arm(args, world: int, rank: int, local: int) -> None:
         extra = workloads.uniform_cubes(info["indices"][-1] + 1, seed=20)
         sample = workloads.uniform_cubes(args.tune_cubes, seed=args.seed + 1000) + \
             [extra[i] for i in info["indices"][n_hard:n_hard + args.tune_hard]]
-        tuned = solver.autotune(sample, save=False, budget_s=args.tune_budget)
+        tuned = solver.autotune(sample, save=False, budget_s=args.tune_budget, target_n=args.batch)
     opts = solver._opts(n=args.batch)
 
     for _ in range(args.warmup):

@@ -135,6 +135,7 @@ class GpuSolver:
         self.last_probes = 0
         self.variant = 0  # search kernel variant (libccs); 0 lets the library choose by batch size
         self.tuned: dict | None = None  # settings chosen by autotune(); else the cached ones
+        self.tuned_bucket: str | None = None  # the batch-size bucket they were measured on
         self.use_autotune = True
         self.second_kind: str | None = None  # kind of the attached second table (table id 1)
         self.flip_rule = FLIP_RULE
@@ -174,10 +175,12 @@ class GpuSolver:
         blocks_per_sm = max(1, round(self.grid / self.sms)) if self.grid else 0
         o = native.solve_opts(self.prefix_len, self.deeper_prefix_at[:2], blocks_per_sm, 0, timeout_s,
                               variant=self.variant, few_divisor=1 if self.exact_thresholds else 0)
-        tuned = self.tuned if self.tuned is not None else None
-        if tuned is None and self.use_autotune:
-            from cuda_cube_solver import autotune
+        from cuda_cube_solver import autotune
 
+        # tuned settings hold for the batch-size bucket they were measured on (a setting chosen
+        # for thousands of cubes is not the one for a lone cube); other sizes keep the defaults
+        tuned = self.tuned if self.tuned is not None and autotune.batch_bucket(n or 1) == self.tuned_bucket else None
+        if tuned is None and self.use_autotune:
             tuned = autotune.lookup(self.table_name, n or 1, self.handle.device)
         if tuned:
             o.variant, o.base_plen, o.spread = tuned["variant"], tuned["base_plen"], tuned["spread"]
@@ -190,16 +193,20 @@ class GpuSolver:
     def table_name(self) -> str:
         return self.kind.name if self.table_format == "block" else f"{self.kind.name}-b3"
 
-    def autotune(self, sample: list[CubieState], log=None, save: bool = True, budget_s: float = 0.0) -> dict:
+    def autotune(self, sample: list[CubieState], log=None, save: bool = True, budget_s: float = 0.0,
+                 target_n: int | None = None) -> dict:
         """Measure the kernel settings on ``sample`` and use the best from now on (within
-        ``budget_s`` seconds when it is > 0)."""
+        ``budget_s`` seconds when it is > 0) for batches of ``target_n`` cubes' size bucket
+        (default: the sample's own size)."""
 
         from cuda_cube_solver import autotune
 
         result = autotune.tune(self.handle, sample, self.table_name, log=log, budget_s=budget_s)
+        n = target_n or len(sample)
         self.tuned = result["config"]
+        self.tuned_bucket = autotune.batch_bucket(n)
         if save:
-            autotune.save(result, self.table_name, len(sample), self.handle.device)
+            autotune.save(result, self.table_name, n, self.handle.device)
         return result
 
     def root_h(self, states: list[CubieState]) -> tuple[np.ndarray, np.ndarray]:
