@@ -50,11 +50,14 @@ struct QueueState {
     unsigned long long admit_head;   // admission ring: cubes waiting for a first iteration
     unsigned long long admit_tail;
     uint32_t yield;                  // host asks lanes to stop fetching new items
-    uint32_t starving;               // set by a lane that found no item and no donated subtree
-    unsigned long long donated;      // subtrees donated (diagnostic)
-    uint32_t don_count;              // donated subtrees waiting in the donation cells
     uint32_t pad;
     unsigned long long scan_pos;     // rotating start of the stranded-cube check
+    // Work-stealing words, on a cache line of their own: idle lanes poll them, and on the line of
+    // the counters above their reads would queue behind every lane's atomics.
+    alignas(128) uint32_t starving;  // set by a lane that found no item and no donated subtree
+    uint32_t don_count;              // donated subtrees waiting in the donation cells
+    unsigned long long donated;      // subtrees donated (diagnostic)
+    uint32_t pad2[28];
 };
 
 // A donated subtree: the unexplored children of one node of a running item (the node at depth g0

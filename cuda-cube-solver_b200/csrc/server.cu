@@ -178,10 +178,16 @@ constexpr uint32_t SERVER_MAX_SLOTS = 65536;
 template <int MODE, int NEC>
 int kernel_footprint_kind(ccs_handle* h, int variant, size_t* local_bytes, int* threads);
 
+// The automatic server shape is 256 x 2 with sibling lookahead (variant 2): on B200 at 200
+// requests/s with 1% superflips it sustained 64 cubes/s against 55 for 256 x 3.
+static int server_variant(const ccs_solve_opts* opts) {
+    return opts && opts->variant > 0 ? resolve_variant(opts, 0) : 2;
+}
+
 // Device memory the server holds whatever the number of cubes: resident tables, constants,
 // prefix lists, queue state, donation cells and the persistent launch's per-lane stacks.
 int server_fixed_bytes(ccs_handle* h, const ccs_solve_opts* opts, uint64_t* out) {
-    const int variant = resolve_variant(opts, 0);
+    const int variant = server_variant(opts);
     const int grid = grid_for(h, opts, variant);
     size_t local = 0;
     int threads = 0;
@@ -254,9 +260,17 @@ extern "C" int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* 
     // stream's p50 rose from 43 to 131 ms on B200 (it pays off for a lone batch or plain solve).
     s->P.few_max_active = 0;
     s->P.idle_limit = 1u << 16;  // ~0.25 s of idle polling, then the launch ends (relaunched on demand)
+    // Work stealing is off for served streams unless asked for (opts->steal 1 or 2): lanes that
+    // find the queue momentarily empty take donated pieces of a long cube ahead of the items of
+    // new arrivals.  Measured on B200 (256 x 3) at 200 requests/s with 1% superflips: uniform
+    // cubes' p95 latency 4.5 s without, 8.8 s with (sustained 55 and 61 cubes/s).
+    if (!(opts && opts->steal > 0)) {
+        s->P.don = nullptr;
+        s->P.don_cap = 0;
+    }
     s->P.done_log = s->d_done_log;
     s->P.done_log_cap = s->log_cap;
-    s->variant = resolve_variant(opts, 0);
+    s->variant = server_variant(opts);
     s->grid = grid_for(h, opts, s->variant);
     QueueState q;
     std::memset(&q, 0, sizeof q);

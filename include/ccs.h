@@ -144,8 +144,9 @@ typedef struct ccs_solve_opts {
     int probe_min;            /* a warp keeps probing (pruned children -> next sibling) while  */
                               /*   at least this many lanes have a probe (0: default, > 32: off) */
     int steal;                /* work stealing: lanes donate unexplored subtrees to idle lanes  */
-                              /*   (phase-ordered variants 1-3, 6-8; 0 or 1: on, asked for by   */
-                              /*   any idle lane; 2: on, asked for by whole idle warps; < 0: off) */
+                              /*   (phase-ordered variants; 0 or 1: on, asked for by any idle   */
+                              /*   lane; 2: on, asked for by whole idle warps; < 0: off).  The  */
+                              /*   server takes 0 as off and steals only with 1 or 2.           */
     int steal_depth;          /* a donated node's slack -- moves to the bound beyond its largest */
                               /*   frame bound -- is at least this (0: 2)                       */
     int steal_period;         /* a lane with work checks for starving lanes every this many    */
