@@ -291,22 +291,17 @@ __global__ void __launch_bounds__(256) encode_block(const uint8_t* __restrict__ 
 // its 2-bit block and mod-3 tables: exact up to the 124-block minimum + 5, otherwise the
 // smallest value >= minimum + 3 with the right residue.  Per 155-entry block: minimum m, cut
 // c in 0..3 maximising the sum of the encoded bounds (lowest c on ties), header m | c << 6, then
-// five base-3 digits per byte (least significant = first entry).
-__global__ void __launch_bounds__(128) encode_b3(const uint8_t* __restrict__ depth, const uint32_t* __restrict__ blk,
-                                                 uint64_t n_entries, uint64_t n_blocks, uint32_t* __restrict__ out) {
-    uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (b >= n_blocks) return;
+// five base-3 digits per byte (least significant = first entry).  `value(x)` gives entry x's
+// value; the two sources below are the exact-depth array and the mod-3 + block tables.
+template <class Value>
+__device__ __forceinline__ void encode_b3_block(uint64_t b, uint64_t n_entries, Value value, uint32_t* __restrict__ out) {
     uint64_t first = b * 155u;
     uint32_t n = (uint32_t)min((uint64_t)155u, n_entries - first);
     unsigned char v[155];
     uint32_t m = 255;
     for (uint32_t j = 0; j < n; ++j) {
-        uint64_t x = first + j;
-        uint32_t dx = depth[x];
-        uint32_t m124 = __ldg(blk + (x / 124u) * 8u) & 0xFFu;
-        uint32_t val = dx <= m124 + 5u ? dx : m124 + 3u + (dx - m124 - 3u) % 3u;
-        v[j] = (unsigned char)val;
-        m = min(m, val);
+        v[j] = (unsigned char)value(first + j);
+        m = min(m, (uint32_t)v[j]);
     }
     uint32_t best = 0, best_score = 0;
     for (uint32_t c = 0; c < 4; ++c) {
@@ -328,6 +323,108 @@ __global__ void __launch_bounds__(128) encode_b3(const uint8_t* __restrict__ dep
     uint32_t* o = out + b * 8u;
     for (int w = 0; w < 8; ++w)
         o[w] = bytes[4 * w] | (bytes[4 * w + 1] << 8) | (bytes[4 * w + 2] << 16) | ((uint32_t)bytes[4 * w + 3] << 24);
+}
+
+__global__ void __launch_bounds__(128) encode_b3(const uint8_t* __restrict__ depth, const uint32_t* __restrict__ blk,
+                                                 uint64_t n_entries, uint64_t n_blocks, uint32_t* __restrict__ out) {
+    uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (b >= n_blocks) return;
+    encode_b3_block(b, n_entries, [&](uint64_t x) -> uint32_t {
+        uint32_t dx = depth[x];
+        uint32_t m124 = __ldg(blk + (x / 124u) * 8u) & 0xFFu;
+        return dx <= m124 + 5u ? dx : m124 + 3u + (dx - m124 - 3u) % 3u;
+    }, out);
+}
+
+// The same file from the reference's two tables (build_b3_table, table.py:52-79): a block offset
+// below 3 gives the value; offset 3 (at least minimum + 3) takes the smallest value >= minimum + 3
+// whose residue is the mod-3 table's -- the exact depth when it is at most minimum + 5.
+__global__ void __launch_bounds__(128) encode_b3_mod3(const uint32_t* __restrict__ mod3, const uint32_t* __restrict__ blk,
+                                                      uint64_t n_entries, uint64_t n_blocks, uint32_t* __restrict__ out) {
+    uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (b >= n_blocks) return;
+    encode_b3_block(b, n_entries, [&](uint64_t x) -> uint32_t {
+        const uint64_t sec = x / 124u;
+        const uint32_t j = (uint32_t)(x - sec * 124u), pos = 8u + 2u * j;
+        const uint32_t m124 = __ldg(blk + sec * 8u) & 0xFFu;
+        const uint32_t off = (__ldg(blk + sec * 8u + (pos >> 5)) >> (pos & 31u)) & 3u;
+        if (off < 3u) return m124 + off;
+        const uint32_t r = (__ldg(mod3 + (x >> 4)) >> (2u * (uint32_t)(x & 15u))) & 3u;
+        const uint32_t lo = m124 + 3u;
+        return lo + (r + 3u - lo % 3u) % 3u;
+    }, out);
+}
+
+// Mod-3 file: per little-endian uint32 sixteen entries, two bits each, depth mod 3 (3 for an
+// unvisited entry and past the end, as the reference's table starts all ones; table.py:94-95).
+__global__ void __launch_bounds__(256) encode_mod3(const uint8_t* __restrict__ depth, uint64_t n_words,
+                                                   uint32_t* __restrict__ out) {
+    const uint4* chunks = reinterpret_cast<const uint4*>(depth);  // 16 depth bytes per output word
+    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < n_words; w += (uint64_t)gridDim.x * blockDim.x) {
+        uint4 v = chunks[w];
+        uint32_t in[4] = {v.x, v.y, v.z, v.w}, word = 0;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            uint32_t d = (in[q >> 2] >> (8 * (q & 3))) & 0xFFu;
+            word |= (d == 0xFFu ? 3u : d % 3u) << (2 * q);
+        }
+        out[w] = word;
+    }
+}
+
+// Base-3 digit of entry j of a sector: byte 1 + j / 5, place j % 5 (least significant first).
+__device__ __forceinline__ uint32_t decode_digit_b3(const uint32_t w[8], uint32_t j) {
+    const uint32_t q = 1u + j / 5u, k = j % 5u;
+    const uint32_t byte = (w[q >> 2] >> (8u * (q & 3u))) & 0xFFu;
+    const uint32_t pw = k == 0 ? 1u : k == 1 ? 3u : k == 2 ? 9u : k == 3 ? 27u : 81u;
+    return (byte / pw) % 3u;
+}
+
+// Entries of a solving table per decoded value (bins[0 .. n_bins-1], the last also holding larger
+// values).  Block sectors are counted with popcounts: offset k of the valid entries goes to bin
+// minimum + k; base-3 sectors per digit (0 -> m, 1 -> m + cut + 1, 2 -> m + cut + 2).
+template <int FMT>
+__global__ void __launch_bounds__(256) table_histogram(const uint32_t* __restrict__ tab, uint64_t n_entries,
+                                                       uint32_t n_bins, unsigned long long* __restrict__ bins) {
+    __shared__ unsigned long long sh[64];
+    for (uint32_t i = threadIdx.x; i < 64; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    constexpr uint32_t PER = SectorTraits<FMT>::PER;
+    const uint64_t n_sec = (n_entries + PER - 1) / PER;
+    for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < n_sec; s += (uint64_t)gridDim.x * blockDim.x) {
+        const uint4* p = reinterpret_cast<const uint4*>(tab + s * 8u);
+        const uint4 a = p[0], c = p[1];
+        const uint32_t w[8] = {a.x, a.y, a.z, a.w, c.x, c.y, c.z, c.w};
+        const uint32_t n = (uint32_t)min((uint64_t)PER, n_entries - s * PER);
+        uint32_t cnt[4] = {0, 0, 0, 0}, base[4];
+        if (FMT == FMT_BLOCK) {
+            // entry j's offset sits at bits 8 + 2j; word i holds entries [16i - 4, 16i + 12)
+            for (int i = 0; i < 8; ++i) {
+                const int j0 = 16 * i - 4;  // entry of the word's bit 0
+                uint32_t valid = 0;
+                for (int t = 0; t < 16; ++t) {
+                    const int j = j0 + t;
+                    if (j >= 0 && j < (int)n) valid |= 1u << (2 * t);
+                }
+                const uint32_t lo = w[i] & valid, hi = (w[i] >> 1) & valid;
+                cnt[1] += __popc(lo & ~hi);
+                cnt[2] += __popc(hi & ~lo);
+                cnt[3] += __popc(lo & hi);
+            }
+            cnt[0] = n - cnt[1] - cnt[2] - cnt[3];
+            const uint32_t m = w[0] & 0xFFu;
+            for (int k = 0; k < 4; ++k) base[k] = m + k;
+        } else {
+            for (uint32_t j = 0; j < n; ++j) cnt[decode_digit_b3(w, j)] += 1;
+            const uint32_t m = w[0] & 63u, cut = (w[0] >> 6) & 3u;
+            base[0] = m, base[1] = m + cut + 1u, base[2] = m + cut + 2u, base[3] = 0;
+        }
+        for (int k = 0; k < 4; ++k)
+            if (cnt[k]) atomicAdd(&sh[min(base[k], n_bins - 1u)], (unsigned long long)cnt[k]);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n_bins; i += blockDim.x)
+        if (sh[i]) atomicAdd(&bins[i], sh[i]);
 }
 
 }  // namespace ccs

@@ -47,6 +47,11 @@ struct DeviceBuffer {
         if (p) cudaFree(p);
     }
     bool ok() const { return p != nullptr; }
+    T* release() {  // the caller owns the allocation from here on (cudaFree)
+        T* q = p;
+        p = nullptr;
+        return q;
+    }
     DeviceBuffer(const DeviceBuffer&) = delete;
     DeviceBuffer& operator=(const DeviceBuffer&) = delete;
 };

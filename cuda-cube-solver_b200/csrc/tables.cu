@@ -209,12 +209,12 @@ extern "C" int ccs_last_build_passes(ccs_handle* h, ccs_bfs_pass* out, int max_o
     return CCS_OK;
 }
 
-extern "C" int ccs_build_table(ccs_handle* h, const char* kind, int format, const char* out_path, int keep_resident,
-                               uint64_t* depth_counts, int max_depths, int* n_depths, double* seconds,
-                               ccs_log_fn log) {
-    if (!h || !kind) return fail(CCS_E_ARG, "NULL argument");
-    if (format != CCS_FMT_BLOCK && format != CCS_FMT_B3) return fail(CCS_E_ARG, "unknown table format %d", format);
-    const std::string first_kind = h->kind_name;  // restored after building a second table
+// One BFS of `kind`, then the files of paths[CCS_FMT_BLOCK / _B3 / _MOD3] (NULL: not written) and,
+// with keep_resident, the table of keep_format kept on the device (1: as the table, 2: as the
+// second table).
+static int build_impl(ccs_handle* h, const char* kind, const char* const paths[3], int keep_format, int keep_resident,
+                      uint64_t* depth_counts, int max_depths, int* n_depths, double* seconds, ccs_log_fn log) {
+    const std::string first_kind = h->kind_ready ? h->kind_name : std::string();  // restored when a table stays
     CCS_TRY(set_kind(h, kind));
     CCS_CUDA_TRY(cudaSetDevice(h->device));
     const KindDesc k = h->kind;
@@ -323,53 +323,152 @@ extern "C" int ccs_build_table(ccs_handle* h, const char* kind, int format, cons
         }
     }
 
-    // Encode the solving file.
+    // Encode: the block table always (the base-3 encoder reads its minima), the base-3 table when
+    // it is written or kept, then the mod-3 file; each file through "<path>.tmp" and a rename.
     const uint64_t n_blk = (n_entries + BLOCK_ENTRIES - 1) / BLOCK_ENTRIES;
-    uint32_t* d_blk = nullptr;
-    if (cudaMalloc(&d_blk, n_blk * 32) != cudaSuccess) return fail(CCS_E_NOMEM, "block table allocation");
-    encode_block<<<h->sms * 8, 256, 0, h->stream>>>(depth.p, n_entries, n_blk, d_blk);
-    cudaError_t e = cudaGetLastError();
-    uint32_t* d_out = d_blk;
-    uint64_t out_bytes = n_blk * 32;
-    if (e == cudaSuccess && format == CCS_FMT_B3) {
-        const uint64_t n_b3 = (n_entries + B3_ENTRIES - 1) / B3_ENTRIES;
-        uint32_t* d_b3 = nullptr;
-        if (cudaMalloc(&d_b3, n_b3 * 32) != cudaSuccess) {
-            cudaFree(d_blk);
-            return fail(CCS_E_NOMEM, "base-3 table allocation");
-        }
-        encode_b3<<<(unsigned)((n_b3 + 127) / 128), 128, 0, h->stream>>>(depth.p, d_blk, n_entries, n_b3, d_b3);
-        e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-        cudaFree(d_blk);
-        d_out = d_b3;
-        out_bytes = n_b3 * 32;
+    const uint64_t n_b3 = (n_entries + B3_ENTRIES - 1) / B3_ENTRIES;
+    DeviceBuffer<uint32_t> blk(n_blk * 8);
+    if (!blk.ok()) return fail(CCS_E_NOMEM, "block table allocation");
+    encode_block<<<h->sms * 8, 256, 0, h->stream>>>(depth.p, n_entries, n_blk, blk.p);
+    CCS_CUDA_TRY(cudaGetLastError());
+    const bool want_b3 = paths[CCS_FMT_B3] || (keep_resident && keep_format == CCS_FMT_B3);
+    DeviceBuffer<uint32_t> b3(want_b3 ? n_b3 * 8 : 0);
+    if (want_b3) {
+        if (!b3.ok()) return fail(CCS_E_NOMEM, "base-3 table allocation");
+        encode_b3<<<(unsigned)((n_b3 + 127) / 128), 128, 0, h->stream>>>(depth.p, blk.p, n_entries, n_b3, b3.p);
+        CCS_CUDA_TRY(cudaGetLastError());
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    if (e != cudaSuccess) {
-        cudaFree(d_out);
-        return fail(CCS_E_CUDA, "encoding the table: %s", cudaGetErrorString(e));
-    }
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return fail(CCS_E_CUDA, "encoding the table: %s", cudaGetErrorString(e));
     double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (seconds) *seconds = secs;
     if (n_depths) *n_depths = (int)counts.size();
     if (depth_counts)
         for (int i = 0; i < (int)counts.size() && i < max_depths; ++i) depth_counts[i] = counts[i];
 
+    if (paths[CCS_FMT_MOD3]) {
+        DeviceBuffer<uint32_t> mod3(n_chunks);
+        if (!mod3.ok()) return fail(CCS_E_NOMEM, "mod-3 table allocation");
+        encode_mod3<<<h->sms * 8, 256, 0, h->stream>>>(depth.p, n_chunks, mod3.p);
+        CCS_CUDA_TRY(cudaGetLastError());
+        CCS_TRY(write_device_file(mod3.p, n_chunks * 4, paths[CCS_FMT_MOD3], h->stream));
+    }
+    if (paths[CCS_FMT_BLOCK]) CCS_TRY(write_device_file(blk.p, n_blk * 32, paths[CCS_FMT_BLOCK], h->stream));
+    if (paths[CCS_FMT_B3]) CCS_TRY(write_device_file(b3.p, n_b3 * 32, paths[CCS_FMT_B3], h->stream));
+
     int rc = CCS_OK;
-    if (out_path) rc = write_device_file(d_out, out_bytes, out_path, h->stream);
-    if (rc == CCS_OK && keep_resident == 1) {
-        free_table(h);
-        h->d_table = d_out;
-        h->table_bytes = out_bytes;
-        h->format = format;
-    } else if (rc == CCS_OK && keep_resident == 2) {
-        std::string second = h->kind_name;
-        rc = set_kind(h, first_kind.c_str());  // the constants stay those of the first table's kind
-        if (rc == CCS_OK) rc = attach_second(h, second.c_str(), format, d_out, out_bytes);
-        if (rc != CCS_OK) cudaFree(d_out);
-    } else {
-        cudaFree(d_out);
+    if (keep_resident == 1 || keep_resident == 2) {
+        DeviceBuffer<uint32_t>& kept = keep_format == CCS_FMT_B3 ? b3 : blk;
+        const uint64_t kept_bytes = keep_format == CCS_FMT_B3 ? n_b3 * 32 : n_blk * 32;
+        uint32_t* d_out = kept.release();
+        if (keep_resident == 1) {
+            free_table(h);
+            h->d_table = d_out;
+            h->table_bytes = kept_bytes;
+            h->format = keep_format;
+        } else {
+            std::string second = h->kind_name;
+            rc = set_kind(h, first_kind.c_str());  // the constants stay those of the first table's kind
+            if (rc == CCS_OK) rc = attach_second(h, second.c_str(), keep_format, d_out, kept_bytes);
+            if (rc != CCS_OK) cudaFree(d_out);
+        }
+    } else if (h->d_table && !first_kind.empty()) {
+        rc = set_kind(h, first_kind.c_str());  // a resident table keeps its kind's constants
     }
     return rc;
+}
+
+extern "C" int ccs_build_table(ccs_handle* h, const char* kind, int format, const char* out_path, int keep_resident,
+                               uint64_t* depth_counts, int max_depths, int* n_depths, double* seconds,
+                               ccs_log_fn log) {
+    if (!h || !kind) return fail(CCS_E_ARG, "NULL argument");
+    if (format != CCS_FMT_BLOCK && format != CCS_FMT_B3) return fail(CCS_E_ARG, "unknown table format %d", format);
+    const char* paths[3] = {nullptr, nullptr, nullptr};
+    paths[format] = out_path;
+    return build_impl(h, kind, paths, format, keep_resident, depth_counts, max_depths, n_depths, seconds, log);
+}
+
+extern "C" int ccs_build_table_files(ccs_handle* h, const char* kind, const char* block_path, const char* b3_path,
+                                     const char* mod3_path, uint64_t* depth_counts, int max_depths, int* n_depths,
+                                     double* seconds, ccs_log_fn log) {
+    if (!h || !kind) return fail(CCS_E_ARG, "NULL argument");
+    if (!block_path && !b3_path && !mod3_path) return fail(CCS_E_ARG, "no file to write");
+    const char* paths[3] = {block_path, b3_path, mod3_path};
+    return build_impl(h, kind, paths, CCS_FMT_BLOCK, 0, depth_counts, max_depths, n_depths, seconds, log);
+}
+
+// Opens `path` and checks that it holds exactly `want` bytes.
+static int open_sized(const char* path, uint64_t want, FILE** out) {
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(CCS_E_FILE, "%s not found", path);
+    fseek(f, 0, SEEK_END);
+    long long size = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    if (size < 0 || (uint64_t)size != want) {
+        fclose(f);
+        return fail(CCS_E_FILE, "%s: size %lld, expected %llu", path, size, (unsigned long long)want);
+    }
+    *out = f;
+    return CCS_OK;
+}
+
+static int read_sized(ccs_handle* h, const char* path, uint64_t n_bytes, DeviceBuffer<uint32_t>& d) {
+    FILE* f = nullptr;
+    CCS_TRY(open_sized(path, n_bytes, &f));
+    const int rc = read_file_to_device(f, d.p, n_bytes, path, h->stream);
+    fclose(f);
+    return rc;
+}
+
+extern "C" int ccs_encode_b3_file(ccs_handle* h, const char* kind, const char* mod3_path, const char* block_path,
+                                  const char* b3_path) {
+    if (!h || !kind || !mod3_path || !block_path || !b3_path) return fail(CCS_E_ARG, "NULL argument");
+    KindDesc k;
+    CCS_TRY(get_kind(kind, &k));
+    CCS_CUDA_TRY(cudaSetDevice(h->device));
+    const uint64_t n_entries = k.n_entries;
+    const uint64_t n_words = (n_entries + 15) / 16;
+    const uint64_t n_blk = (n_entries + BLOCK_ENTRIES - 1) / BLOCK_ENTRIES;
+    const uint64_t n_b3 = (n_entries + B3_ENTRIES - 1) / B3_ENTRIES;
+    DeviceBuffer<uint32_t> mod3(n_words), blk(n_blk * 8), b3(n_b3 * 8);
+    if (!mod3.ok() || !blk.ok() || !b3.ok()) return fail(CCS_E_NOMEM, "device allocation for the base-3 encoding");
+    CCS_TRY(read_sized(h, mod3_path, n_words * 4, mod3));
+    CCS_TRY(read_sized(h, block_path, n_blk * 32, blk));
+    encode_b3_mod3<<<(unsigned)((n_b3 + 127) / 128), 128, 0, h->stream>>>(mod3.p, blk.p, n_entries, n_b3, b3.p);
+    CCS_CUDA_TRY(cudaGetLastError());
+    CCS_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return write_device_file(b3.p, n_b3 * 32, b3_path, h->stream);
+}
+
+extern "C" int ccs_save_table(ccs_handle* h, int table, const char* path) {
+    if (!h || !path) return fail(CCS_E_ARG, "NULL argument");
+    if (table != 0 && table != 1) return fail(CCS_E_ARG, "table %d: 0 or 1", table);
+    const uint32_t* d = table ? h->d_table2 : h->d_table;
+    const uint64_t n = table ? h->table2_bytes : h->table_bytes;
+    if (!d) return fail(CCS_E_STATE, "no table %d loaded", table);
+    CCS_CUDA_TRY(cudaSetDevice(h->device));
+    return write_device_file(d, n, path, h->stream);
+}
+
+extern "C" int ccs_table_histogram(ccs_handle* h, int table, uint64_t* bins, int n_bins) {
+    if (!h || !bins) return fail(CCS_E_ARG, "NULL argument");
+    if (table != 0 && table != 1) return fail(CCS_E_ARG, "table %d: 0 or 1", table);
+    if (n_bins < 1 || n_bins > 64) return fail(CCS_E_ARG, "n_bins %d: 1 to 64", n_bins);
+    const uint32_t* d = table ? h->d_table2 : h->d_table;
+    if (!d) return fail(CCS_E_STATE, "no table %d loaded", table);
+    CCS_CUDA_TRY(cudaSetDevice(h->device));
+    DeviceBuffer<unsigned long long> out(64);
+    if (!out.ok()) return fail(CCS_E_NOMEM, "histogram buffer");
+    CCS_CUDA_TRY(cudaMemsetAsync(out.p, 0, 64 * 8, h->stream));
+    // both tables share the kind's entry count (a second table matches the first's kind family)
+    if (h->format == CCS_FMT_B3)
+        table_histogram<FMT_B3><<<h->sms * 4, 256, 0, h->stream>>>(d, h->kind.n_entries, (uint32_t)n_bins, out.p);
+    else
+        table_histogram<FMT_BLOCK><<<h->sms * 4, 256, 0, h->stream>>>(d, h->kind.n_entries, (uint32_t)n_bins, out.p);
+    CCS_CUDA_TRY(cudaGetLastError());
+    unsigned long long hb[64];
+    CCS_CUDA_TRY(cudaMemcpyAsync(hb, out.p, sizeof hb, cudaMemcpyDeviceToHost, h->stream));
+    CCS_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (int i = 0; i < n_bins; ++i) bins[i] = hb[i];
+    return CCS_OK;
 }

@@ -97,6 +97,11 @@ _SIGS = {
     "ccs_load_table": [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p],
     "ccs_build_table": [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
                         ctypes.c_void_p, ctypes.c_int, _P(ctypes.c_int), _P(ctypes.c_double), LOG_FN],
+    "ccs_build_table_files": [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                              ctypes.c_void_p, ctypes.c_int, _P(ctypes.c_int), _P(ctypes.c_double), LOG_FN],
+    "ccs_encode_b3_file": [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p],
+    "ccs_save_table": [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p],
+    "ccs_table_histogram": [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int],
     "ccs_table_bytes": [ctypes.c_void_p, _P(ctypes.c_uint64)],
     "ccs_table_copy": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64],
     "ccs_index": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
@@ -226,6 +231,30 @@ class Handle:
                                   None if out_path is None else str(out_path).encode(), int(keep_resident),
                                   _ptr(counts), 64, ctypes.byref(n), ctypes.byref(secs), cb))
         return [int(c) for c in counts[:n.value]], secs.value
+
+    def build_table_files(self, kind: str, block_path=None, b3_path=None, mod3_path=None, log=None):
+        """One BFS writing each given file (block, base-3, the reference's mod-3); returns
+        (per-depth counts, seconds).  The resident tables are left as they are."""
+        counts = np.zeros(64, np.uint64)
+        n = ctypes.c_int()
+        secs = ctypes.c_double()
+        cb = LOG_FN(lambda m: log(m.decode())) if log else LOG_FN()
+        enc = (lambda p: None if p is None else str(p).encode())
+        check(lib.ccs_build_table_files(self._h, kind.encode(), enc(block_path), enc(b3_path), enc(mod3_path),
+                                        _ptr(counts), 64, ctypes.byref(n), ctypes.byref(secs), cb))
+        return [int(c) for c in counts[:n.value]], secs.value
+
+    def encode_b3_file(self, kind: str, mod3_path, block_path, b3_path) -> None:
+        check(lib.ccs_encode_b3_file(self._h, kind.encode(), str(mod3_path).encode(), str(block_path).encode(),
+                                     str(b3_path).encode()))
+
+    def save_table(self, path, table: int = 0) -> None:
+        check(lib.ccs_save_table(self._h, int(table), str(path).encode()))
+
+    def table_histogram(self, table: int = 0, n_bins: int = 32) -> list[int]:
+        bins = np.zeros(n_bins, np.uint64)
+        check(lib.ccs_table_histogram(self._h, int(table), _ptr(bins), int(n_bins)))
+        return [int(b) for b in bins]
 
     def last_build_passes(self) -> list[dict]:
         """The last build's BFS passes: depth, direction, entries found, random reads, claims, seconds."""

@@ -34,6 +34,9 @@ extern "C" {
 
 #define CCS_FMT_BLOCK 0       /* 2-bit block table, "prune-ud-<kind>-blk.bin" */
 #define CCS_FMT_B3 1          /* base-3 block table, "prune-ud-<kind>-b3.bin" */
+#define CCS_FMT_MOD3 2        /* the reference's mod-3 file "prune-ud-<kind>.bin": depth mod 3 in  */
+                              /*   two bits, sixteen entries per little-endian uint32, 3 past the   */
+                              /*   end (table.py:82-129,140-167); written by builds, not solved on  */
 
 typedef struct ccs_handle ccs_handle;
 
@@ -85,6 +88,31 @@ int ccs_load_table(ccs_handle* h, const char* kind, int format, const char* path
  * without the file write).  log may be NULL. */
 int ccs_build_table(ccs_handle* h, const char* kind, int format, const char* out_path, int keep_resident,
                     uint64_t* depth_counts, int max_depths, int* n_depths, double* seconds, ccs_log_fn log);
+
+/* One BFS, several files (table.build, table.py:140-167, which writes the mod-3 and block files
+ * of one generate): each non-NULL path is written from the same exact-depth array, through
+ * "<path>.tmp" and a rename.  The handle's resident tables are left as they are; its kind becomes
+ * `kind` (as after ccs_set_kind).  Counts, seconds and log as for ccs_build_table. */
+int ccs_build_table_files(ccs_handle* h, const char* kind, const char* block_path, const char* b3_path,
+                          const char* mod3_path, uint64_t* depth_counts, int max_depths, int* n_depths,
+                          double* seconds, ccs_log_fn log);
+
+/* Base-3 file from the mod-3 and block files of `kind` (table.build_b3_table and write_b3,
+ * table.py:52-79): both are read onto the device (sizes checked), encoded there, and the base-3
+ * file is written to b3_path (through "<b3_path>.tmp").  The handle's tables are untouched. */
+int ccs_encode_b3_file(ccs_handle* h, const char* kind, const char* mod3_path, const char* block_path,
+                       const char* b3_path);
+
+/* Write a resident table -- table 0, or 1 for the second table -- to a file in chunks through
+ * pinned staging (table.save_device, table.py:20-25), through "<path>.tmp" and a rename. */
+int ccs_save_table(ccs_handle* h, int table, const char* path);
+
+/* Entries of a resident table (0, or 1 for the second) per stored lower bound, counted on the
+ * device: bins[v] = entries whose decoded value is v, the last bin also holding larger values
+ * (table.histogram, table.py:132-137, counts the mod-3 table's four values; the solving tables
+ * hold a bound per entry, so the bins are those bounds: exact below a 2-bit block's minimum + 3,
+ * and "at least" at the cut of either format).  The bins sum to the kind's entry count. */
+int ccs_table_histogram(ccs_handle* h, int table, uint64_t* bins, int n_bins);
 
 /* One BFS pass of the last ccs_build_table: the depth it assigned, forward (1: expand the
  * frontier, kernels.cu:544-574) or backward (0: unvisited entries test their neighbours,

@@ -119,3 +119,119 @@ def test_file_roundtrip_and_size_check(tmp_path):
             h2.load_table("304", "block", tmp_path / "missing.bin")
     finally:
         h2.close()
+
+
+def _block_histogram(words: np.ndarray, n_entries: int, n_bins: int = 32) -> np.ndarray:
+    """Host count of a 2-bit block table's entries per decoded value (minimum + offset)."""
+
+    sec = words.reshape(-1, 8)
+    m = (sec[:, 0] & 0xFF).astype(np.int64)
+    cnt = np.zeros((len(sec), 4), np.int32)
+    last = n_entries - (len(sec) - 1) * 124  # entries in the last sector
+    for i in range(8):
+        j0 = 16 * i - 4  # entry at bit 0 of word i
+        full = sum(1 << (2 * t) for t in range(16) if 0 <= j0 + t < 124)
+        tail = sum(1 << (2 * t) for t in range(16) if 0 <= j0 + t < last)
+        valid = np.full(len(sec), full, np.uint32)
+        valid[-1] = tail
+        lo, hi = sec[:, i] & valid, (sec[:, i] >> 1) & valid
+        cnt[:, 1] += np.bitwise_count(lo & ~hi)
+        cnt[:, 2] += np.bitwise_count(hi & ~lo)
+        cnt[:, 3] += np.bitwise_count(lo & hi)
+    cnt[:, 0] = 124 - cnt[:, 1:].sum(axis=1)
+    cnt[-1, 0] -= 124 - last
+    out = np.zeros(n_bins, np.int64)
+    for k in range(4):
+        out += np.bincount(np.minimum(m + k, n_bins - 1), weights=cnt[:, k], minlength=n_bins).astype(np.int64)
+    return out
+
+
+def _b3_histogram(data: np.ndarray, n_entries: int, n_bins: int = 32) -> np.ndarray:
+    """Host count of a base-3 table's entries per decoded value (digit 0 -> m, 1 -> m + cut + 1,
+    2 -> m + cut + 2)."""
+
+    sec = data.reshape(-1, 32)
+    lut = np.zeros((256, 3), np.uint8)  # digits 0 / 1 / 2 among a byte's five
+    for b in range(243):
+        for k in range(5):
+            lut[b, (b // 3 ** k) % 3] += 1
+    cnt = np.zeros((len(sec), 3), np.int32)
+    for q in range(1, 32):
+        cnt += lut[sec[:, q]]
+    last = n_entries - (len(sec) - 1) * 155
+    cnt[-1, 0] -= 155 - last  # digits past the end are 0
+    m = (sec[:, 0] & 63).astype(np.int64)
+    cut = (sec[:, 0] >> 6).astype(np.int64)
+    out = np.zeros(n_bins, np.int64)
+    for k, base in enumerate((m, m + cut + 1, m + cut + 2)):
+        out += np.bincount(np.minimum(base, n_bins - 1), weights=cnt[:, k], minlength=n_bins).astype(np.int64)
+    return out
+
+
+def test_reference_table_files_and_helpers(tmp_path, depth_golden):
+    """table.build (mod-3 and block files of one BFS), build_b3_table (base 3 from those two files),
+    save_device and histogram on the 304 kind, against the CPU oracle's digests and host decodes."""
+
+    from cuda_cube_solver import table
+
+    golden = _sha_golden()["304"]
+    h = native.Handle()
+    try:
+        mod3 = table.build(tmp_path, "304", log=None, handle=h)
+        meta = json.loads(mod3.with_suffix(".json").read_text())
+        n = meta["entries"]
+        assert meta["depth_counts"] == depth_golden["304"]["depth_counts"]
+        blk = tmp_path / "prune-ud-304-blk.bin"
+        assert _sha(np.fromfile(blk, np.uint8)) == golden["block_sha256"]
+
+        # mod-3 file: residues in 2 bits, 3 past the end; its value counts are the depth counts
+        # folded mod 3 (the reference's build self-check, table.py:146-149)
+        words = np.fromfile(mod3, np.uint32)
+        assert len(words) == (n + 15) // 16
+        lo, hi = words & np.uint32(0x55555555), (words >> 1) & np.uint32(0x55555555)
+        got = [int(np.bitwise_count(~lo & ~hi & np.uint32(0x55555555)).sum()), int(np.bitwise_count(lo & ~hi).sum()),
+               int(np.bitwise_count(hi & ~lo).sum()), int(np.bitwise_count(lo & hi).sum())]
+        counts = meta["depth_counts"]
+        want = [sum(counts[d] for d in range(r, len(counts), 3)) for r in range(3)] + [len(words) * 16 - n]
+        assert got == want
+        # where the block table is exact (offset < 3) its value has the mod-3 file's residue
+        bw = np.fromfile(blk, np.uint32).reshape(-1, 8)
+        x = np.random.default_rng(5).integers(0, n, 200_000, dtype=np.int64)
+        sec, j = x // 124, x % 124
+        pos = 8 + 2 * j
+        off = (bw[sec, pos // 32] >> (pos % 32).astype(np.uint32)) & 3
+        r = (words[x // 16] >> (2 * (x % 16)).astype(np.uint32)) & 3
+        exact = off < 3
+        assert exact.any()
+        assert np.array_equal(((bw[sec, 0] & 0xFF) + off)[exact] % 3, r[exact])
+
+        b3 = table.build_b3_table(tmp_path, "304", handle=h, log=lambda *_: None)
+        b3_bytes = np.fromfile(b3, np.uint8)
+        assert _sha(b3_bytes) == golden["b3_sha256"]  # the same file as the depth-array encoder's
+
+        h.load_table("304", "block", blk)
+        out = tmp_path / "saved-blk.bin"
+        table.save_device(h, out)
+        assert _sha(np.fromfile(out, np.uint8)) == golden["block_sha256"]
+        bins = table.histogram(h)
+        assert sum(bins) == n
+        assert bins == _block_histogram(bw.reshape(-1), n).tolist()
+        assert bins[0] == counts[0]  # the solved entry's block is exact at depth 0
+
+        h.load_table("304", "b3", b3)
+        bins3 = table.histogram(h)
+        assert sum(bins3) == n
+        assert bins3 == _b3_histogram(b3_bytes, n).tolist()
+
+        with pytest.raises(native.CcsError, match="no table 1"):
+            table.save_device(h, tmp_path / "none.bin", table=1)
+        with pytest.raises(native.CcsError, match="n_bins"):
+            h.table_histogram(0, 0)
+        with pytest.raises(native.CcsError, match="no file to write"):
+            h.build_table_files("304")
+        short = tmp_path / "short-mod3.bin"
+        words[:1000].tofile(short)
+        with pytest.raises(native.CcsError, match="size 4000"):
+            table.write_b3(short, blk, "304", tmp_path / "x-b3.bin", handle=h)
+    finally:
+        h.close()
