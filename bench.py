@@ -327,7 +327,12 @@ def bfs_roofline(passes: list[dict], entries: int, peak_gbs: float, ceiling: flo
         out["achieved_gb_s"] = top["achieved_gb_s"]
         out["frac_of_hbm_peak"] = top["achieved_gb_s"] / peak_gbs
         if ceiling:
-            out["frac_of_random_sector_ceiling"] = top["random_sectors_per_s"] / ceiling
+            # Neighbours of nearby entries share classes, so most of a pass's random accesses hit
+            # L2: a rate above the DRAM random-sector ceiling says so, it is not a fraction of it.
+            out["random_rate_over_dram_random_ceiling"] = top["random_sectors_per_s"] / ceiling
+            out["note"] = ("random accesses costed as 32-byte sectors; a rate above the search's DRAM "
+                           "random-sector ceiling means most of them hit L2 (profiles/bfs_s4_dram.md: "
+                           "DRAM bytes per pass)")
     return out
 
 

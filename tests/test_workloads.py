@@ -81,4 +81,4 @@ def test_bfs_roofline_arithmetic():
     r = bench.bfs_roofline(passes, entries=1000, peak_gbs=1.0, ceiling=50.0)
     assert r["dominant_pass"] == {"depth": 2, "dir": "bwd", "seconds": 1.5} and r["dominant_share"] == 0.75
     assert r["passes"][0]["algorithmic_gb"] == (1000 + 32 * 16) / 1e9
-    assert abs(r["frac_of_random_sector_ceiling"] - (100 / 1.5) / 50.0) < 1e-12
+    assert abs(r["random_rate_over_dram_random_ceiling"] - (100 / 1.5) / 50.0) < 1e-12
