@@ -202,6 +202,24 @@ def cpu_window(kind: str, fmt: str, table: np.ndarray, cubes, seconds: float, th
             "finished": int(done.sum()), "window_s": dt, "probes_per_s": float(probes.sum()) / dt}
 
 
+def coordinate_model_baseline(kind: str, seconds: float = 3.0) -> dict:
+    """The host Python coordinate model (frames + table index, one cube at a time) on one core and
+    on every core (a spawn pool, one process per core, each for ``seconds``)."""
+
+    import multiprocessing as mp
+
+    from cuda_cube_solver import workloads
+
+    n1, t1 = workloads.coordinate_model_rate(kind, seconds)
+    cores = os.cpu_count() or 1
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.starmap(workloads.coordinate_model_rate, [(kind, seconds, i) for i in range(cores)])
+    return {"source": "cuda_cube_solver.prefixes.frames + coords.table_index (the reference's Python "
+                      "coordinate model restated), one cube at a time", "kind": kind,
+            "indexes_per_s_1": n1 / t1, "indexes_per_s_all": sum(n for n, _ in res) / max(t for _, t in res),
+            "cores": cores, "seconds_per_process": seconds}
+
+
 def reference_cpu_gather(probes_per_cube: float | None) -> dict | None:
     """The reference's own CPU probe benchmark (its bench/cpu_gather.c, compiled from its checkout
     into oracle/_ref/): random byte lookups in a 7.3 GiB buffer on all host threads and on one,
@@ -529,10 +547,11 @@ def main_arm(args, world: int, rank: int, local: int) -> None:
                                              "frac": roofline["probes_per_s"] / ceiling}
 
     cpu = None
-    if not args.no_cpu:
+    if not args.no_cpu and world == 1:  # the host-core baselines: rank 0 at one GPU only
         c = cpu_window(args.kind, args.format, h.table_copy(), cubes[:1024], args.cpu_budget)
         cpu = {k: c[k] for k in ("value", "unit", "cores", "kind", "sample")}
         cpu["reference_cpu_gather"] = reference_cpu_gather(roofline["probes_per_cube"])
+        cpu["python_coordinate_model"] = coordinate_model_baseline(args.kind)
 
     _, entries = native.kind_info(args.kind)
     out = {"metric": METRIC, "value": value, "unit": "cubes/s", "n_gpus": world, "steps": args.steps,

@@ -91,3 +91,25 @@ def batched_mix(n: int = 4096, seed: int = 2, hard_frac: float = 0.05) -> tuple[
         cubes[int(pos)] = cube
         known[int(pos)] = length
     return cubes, known
+
+
+def coordinate_model_rate(kind: str, seconds: float, seed: int = 0) -> tuple[int, float]:
+    """Table indexes the host Python coordinate model computes in about ``seconds`` in this
+    process, one cube at a time: the six frames of a cube (``prefixes.frames``) and the table index
+    of each (``coords.table_index``), as the reference's root bound does in Python
+    (``solver.py:58-64``, ``coords.py:347``).  Returns (indexes, elapsed seconds)."""
+
+    import time
+
+    from cuda_cube_solver import coords, kinds
+    from cuda_cube_solver.prefixes import frames
+
+    k = kinds.get(kind)
+    cubes = uniform_cubes(64, seed=seed)
+    done, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        for f in frames(cubes[(done // 6) % len(cubes)]):
+            coords.table_index(*coords.pack(f), kind=k)
+            done += 1
+    return done, time.perf_counter() - t0
+
