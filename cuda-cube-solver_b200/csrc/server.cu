@@ -260,14 +260,13 @@ extern "C" int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* 
     // stream's p50 rose from 43 to 131 ms on B200 (it pays off for a lone batch or plain solve).
     s->P.few_max_active = 0;
     s->P.idle_limit = 1u << 16;  // ~0.25 s of idle polling, then the launch ends (relaunched on demand)
-    // Work stealing is off for served streams unless asked for (opts->steal 1 or 2): lanes that
-    // find the queue momentarily empty take donated pieces of a long cube ahead of the items of
-    // new arrivals.  Measured on B200 (256 x 3) at 200 requests/s with 1% superflips: uniform
-    // cubes' p95 latency 4.5 s without, 8.8 s with (sustained 55 and 61 cubes/s).
-    if (!(opts && opts->steal > 0)) {
-        s->P.don = nullptr;
-        s->P.don_cap = 0;
-    }
+    // Served streams steal with whole idle warps asking (opts->steal 0 or 2; 1: any idle lane
+    // asks; < 0: off).  With any idle lane asking, a lane whose bounded ring scan came up empty
+    // asks even while the ring still holds items, which under overload is often.  Measured on
+    // B200 (256 x 2 with lookahead; 90% uniform, 9% of length >= 18, 1% superflips): sustained
+    // 86.8 / 51.3 cubes/s at 100 / 200 requests/s with whole warps asking, 75.4 / 51.2 without
+    // stealing, 75.2 / 20.9 with any lane asking.
+    if (!opts || opts->steal == 0) s->P.don_eager = 0u;
     s->P.done_log = s->d_done_log;
     s->P.done_log_cap = s->log_cap;
     s->variant = server_variant(opts);

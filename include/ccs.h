@@ -174,7 +174,7 @@ typedef struct ccs_solve_opts {
     int steal;                /* work stealing: lanes donate unexplored subtrees to idle lanes  */
                               /*   (phase-ordered variants; 0 or 1: on, asked for by any idle   */
                               /*   lane; 2: on, asked for by whole idle warps; < 0: off).  The  */
-                              /*   server takes 0 as off and steals only with 1 or 2.           */
+                              /*   server takes 0 as 2 (whole idle warps ask).                  */
     int steal_depth;          /* a donated node's slack -- moves to the bound beyond its largest */
                               /*   frame bound -- is at least this (0: 2)                       */
     int steal_period;         /* a lane with work checks for starving lanes every this many    */
