@@ -224,13 +224,17 @@ __device__ __forceinline__ bool server_idle(const SearchParams& P) {
     return q->active == 0u && q->admit_head >= q->admit_tail;
 }
 
-// Keeps the ring's head moving so that the queued positions (tail - head) stay well under the
-// capacity: retired entries are passed, and once the ring is half full a live entry at the head
-// (a cube whose long iteration is still being handed out) is moved to the tail instead of holding
-// every later position behind it.  Entries are plain slot references, so a moved one serves the
-// same iteration from its new place.
+// Keeps the ring's head moving: retired entries are passed, and once the queued positions (tail -
+// head) reach a limit a live entry at the head (a cube whose long iteration is still being handed
+// out) is moved to the tail instead of holding every later position behind it.  Entries are plain
+// slot references, so a moved one serves the same iteration from its new place.  Lanes start
+// their scans within the first `spread` positions after the head, so a server launch keeps the
+// queue within half of that: otherwise, behind one long-lived entry, the entries of cubes that
+// arrive later fall out of every lane's reach until that entry is handed out.  A batch launch
+// keeps its entries in place until the ring is half full.
 static __device__ __noinline__ void advance_head(const SearchParams& P) {
     volatile QueueState* q = P.q;
+    const unsigned long long limit = P.persistent ? (P.spread / 2u > 32u ? P.spread / 2u : 32u) : P.ring_cap / 2u;
     for (int a = 0; a < 4; ++a) {
         unsigned long long h = q->head, t = q->tail;
         if (h >= t) return;
@@ -239,7 +243,7 @@ static __device__ __noinline__ void advance_head(const SearchParams& P) {
         unsigned long long lap = e >> 32, want = h / P.ring_cap;
         if (lap < want || lap == 0xFFFFFFFFull) return;  // reserved by an enqueue, not yet written
         if (lap == want && (uint32_t)e != RING_RETIRED) {
-            if (t - h < P.ring_cap / 2u) return;  // room left: the live entry stays
+            if (t - h < limit) return;  // within the limit: the live entry stays
             if (atomicCAS(cell, e, (e & 0xFFFFFFFF00000000ull) | RING_RETIRED) != e) return;
             enqueue_entry(P, (uint32_t)e);
         }

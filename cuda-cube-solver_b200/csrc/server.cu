@@ -178,8 +178,10 @@ constexpr uint32_t SERVER_MAX_SLOTS = 65536;
 template <int MODE, int NEC>
 int kernel_footprint_kind(ccs_handle* h, int variant, size_t* local_bytes, int* threads);
 
-// The automatic server shape is 256 x 2 with sibling lookahead (variant 2): on B200 at 200
-// requests/s with 1% superflips it sustained 64 cubes/s against 55 for 256 x 3.
+// The automatic server shape is 256 x 2 with sibling lookahead (variant 2), the low-latency one:
+// on B200 a stream at 10 requests/s has a p50 of 21 ms with it and 46 ms with 256 x 3; at 100
+// requests/s (90% uniform, 9% of length >= 18, 1% superflips) 256 x 3 is ahead (91 cubes/s
+// sustained, p50 94 ms, against 87-89 cubes/s, p50 123-165 ms).
 static int server_variant(const ccs_solve_opts* opts) {
     return opts && opts->variant > 0 ? resolve_variant(opts, 0) : 2;
 }
@@ -261,11 +263,9 @@ extern "C" int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* 
     s->P.few_max_active = 0;
     s->P.idle_limit = 1u << 16;  // ~0.25 s of idle polling, then the launch ends (relaunched on demand)
     // Served streams steal with whole idle warps asking (opts->steal 0 or 2; 1: any idle lane
-    // asks; < 0: off).  With any idle lane asking, a lane whose bounded ring scan came up empty
-    // asks even while the ring still holds items, which under overload is often.  Measured on
-    // B200 (256 x 2 with lookahead; 90% uniform, 9% of length >= 18, 1% superflips): sustained
-    // 86.8 / 51.3 cubes/s at 100 / 200 requests/s with whole warps asking, 75.4 / 51.2 without
-    // stealing, 75.2 / 20.9 with any lane asking.
+    // asks; < 0: off).  Measured on B200 (256 x 2 with lookahead; 90% uniform, 9% of length >= 18,
+    // 1% superflips): sustained 86.8-89.0 cubes/s at 100 requests/s with whole warps asking, 77.8
+    // with any lane asking, 75.4 without stealing.
     if (!opts || opts->steal == 0) s->P.don_eager = 0u;
     s->P.done_log = s->d_done_log;
     s->P.done_log_cap = s->log_cap;
