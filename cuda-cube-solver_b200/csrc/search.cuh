@@ -107,6 +107,8 @@ struct SearchParams {
     uint32_t don_eager;              // 1: a lane without work asks for donations (0: a whole idle warp)
     unsigned long long don_min_prev; // donate for cubes whose previous iteration had >= this many nodes
     uint32_t persistent;             // server: an empty queue is not the end (lanes wait for new cubes)
+    unsigned long long head_limit;   // queued positions (tail - head) past which a live head entry moves
+                                     // to the tail (0: half the ring)
     unsigned long long* done_log;    // host-mapped completion log (server), may be null
     uint32_t done_log_cap;
 };

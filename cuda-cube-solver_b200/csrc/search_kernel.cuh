@@ -228,13 +228,12 @@ __device__ __forceinline__ bool server_idle(const SearchParams& P) {
 // head) reach a limit a live entry at the head (a cube whose long iteration is still being handed
 // out) is moved to the tail instead of holding every later position behind it.  Entries are plain
 // slot references, so a moved one serves the same iteration from its new place.  Lanes start
-// their scans within the first `spread` positions after the head, so a server launch keeps the
-// queue within half of that: otherwise, behind one long-lived entry, the entries of cubes that
-// arrive later fall out of every lane's reach until that entry is handed out.  A batch launch
-// keeps its entries in place until the ring is half full.
+// their scans within the first `spread` positions after the head, so with a limit of half of
+// that (P.head_limit; the server's default) no queued cube falls out of every lane's reach behind
+// one long-lived entry; with P.head_limit 0 the limit is half the ring.
 static __device__ __noinline__ void advance_head(const SearchParams& P) {
     volatile QueueState* q = P.q;
-    const unsigned long long limit = P.persistent ? (P.spread / 2u > 32u ? P.spread / 2u : 32u) : P.ring_cap / 2u;
+    const unsigned long long limit = P.head_limit ? P.head_limit : P.ring_cap / 2u;
     for (int a = 0; a < 4; ++a) {
         unsigned long long h = q->head, t = q->tail;
         if (h >= t) return;

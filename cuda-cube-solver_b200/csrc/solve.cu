@@ -91,6 +91,8 @@ void fill_params(ccs_handle* h, const ccs_solve_opts* o, SearchParams* P) {
     P->don_eager = o && o->steal == 2 ? 0u : 1u;
     P->don_min_prev = o && o->steal_min_nodes != 0 ? (o->steal_min_nodes > 0 ? (unsigned long long)o->steal_min_nodes : 0ull)
                                                    : 10000000ull;
+    // Head rotation at half the scan window (rotate 1) or at half the ring (-1, the batch default).
+    P->head_limit = o && o->rotate > 0 ? std::max<unsigned long long>(P->spread / 2u, 32u) : 0ull;
     P->done_log = nullptr;
     P->done_log_cap = 0;
 }

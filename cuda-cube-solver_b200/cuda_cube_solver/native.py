@@ -55,6 +55,7 @@ class SolveOpts(ctypes.Structure):
         ("steal_target", ctypes.c_int),
         ("few_divisor", ctypes.c_int),
         ("steal_min_nodes", ctypes.c_double),
+        ("rotate", ctypes.c_int),
     ]
 
 
@@ -190,10 +191,11 @@ def solve_opts(base_plen: int = 4, deeper_at: tuple[float, float] = (5e7, 3e9), 
                threads: int = 0, timeout_s: float = 0.0, spread: int = 0, variant: int = 0,
                shallow_at: tuple[float, float] = (0.0, 0.0), move_min: int = 0, move_age: int = 0,
                probe_min: int = 0, steal: int = 0, steal_depth: int = 0, steal_period: int = 0,
-               steal_target: int = 0, few_divisor: int = 0, steal_min_nodes: float = 0.0) -> SolveOpts:
+               steal_target: int = 0, few_divisor: int = 0, steal_min_nodes: float = 0.0,
+               rotate: int = 0) -> SolveOpts:
     return SolveOpts(base_plen, float(deeper_at[0]), float(deeper_at[1]), blocks_per_sm, threads, timeout_s, spread,
                      variant, float(shallow_at[0]), float(shallow_at[1]), move_min, move_age, probe_min, steal,
-                     steal_depth, steal_period, steal_target, few_divisor, float(steal_min_nodes))
+                     steal_depth, steal_period, steal_target, few_divisor, float(steal_min_nodes), int(rotate))
 
 
 class Handle:

@@ -184,6 +184,10 @@ typedef struct ccs_solve_opts {
                               /*   by this (0: 50; 1: never, the reference's plain thresholds)  */
     double steal_min_nodes;   /* subtrees of a cube are donated only once its previous          */
                               /*   iteration reached this many nodes (0: 1e7; < 0: always)      */
+    int rotate;               /* a live entry at the work ring's head moves to the tail once   */
+                              /*   the queue spans half of `spread` (1), or half the ring (-1), */
+                              /*   so every queued cube stays within the lanes' scan window     */
+                              /*   (0: 1 for the server, -1 for ccs_solve)                      */
 } ccs_solve_opts;
 
 typedef struct ccs_result {

@@ -133,6 +133,22 @@ def test_launch_shapes_agree(lengths_golden):
     assert h2d > 64 * 416 and d2h > 64 * 416
 
 
+def test_head_rotation_keeps_lengths_and_iteration_nodes(lengths_golden):
+    """Live ring entries moved from the head to the tail (rotate 1, here with a 64-entry window so
+    that entries move all the time) serve the same iterations: the lengths equal the reference's
+    and every completed iteration has the node count of a search without rotation."""
+
+    h = resident_handle("d4t")
+    cubes = lengths_golden["random1000"][400:431]  # fewer than 32: prefix lengths do not depend on timing
+    words = state_words([_state(parse_moves(c["scramble"])) for c in cubes])
+    base = dict(timeout_s=600, variant=3, deeper_at=(1e18, 1e18), steal=-1, spread=64)
+    plain = h.solve(words, native.solve_opts(rotate=-1, **base))
+    moved = h.solve(words, native.solve_opts(rotate=1, **base))
+    assert [r.length for r in moved] == [r.length for r in plain] == [c["length"] for c in cubes]
+    for a, b in zip(moved, plain):
+        assert list(a.iter_nodes[: a.length]) == list(b.iter_nodes[: b.length])
+
+
 def test_lone_superflip_with_stealing(lengths_golden):
     """A lone hard cube spreads over the GPU through donated subtrees: the superflip on d4t."""
 
