@@ -265,9 +265,11 @@ def reference_table(kind: str, fmt: str, device: int) -> tuple[np.ndarray, float
     return host, secs
 
 
-def reference_gpu_run(kind: str, fmt: str, states, batch: int, device: int) -> dict:
+def reference_gpu_run(kind: str, fmt: str, states, batch: int, device: int, one_per_call: int = 0) -> dict:
     """The reference's kernels.cu on this GPU with its per-bound host loop, ``batch`` cubes per
-    solve call (its CLI default is 100); wall clock, like the reference's own benchmark."""
+    solve call (its CLI default is 100); wall clock, like the reference's own benchmark.  With
+    ``one_per_call``, the first that many cubes are also solved one per call (the plain drop-in's
+    shape), on the same table."""
 
     sys.path.insert(0, str(ROOT / "baseline"))
     import ref_gpu
@@ -286,11 +288,23 @@ def reference_gpu_run(kind: str, fmt: str, states, batch: int, device: int) -> d
             nodes += nd
             lengths.append(len(moves))
     dt = time.perf_counter() - t0
+    one = None
+    if one_per_call:
+        lat, one_len = [], []
+        for s in states[:one_per_call]:
+            t1 = time.perf_counter()
+            (moves, _, _), = solver.solve([s])
+            lat.append(time.perf_counter() - t1)
+            one_len.append(len(moves))
+        one = {"cubes": len(lat), "cubes_per_s": len(lat) / sum(lat), "p50_s": float(np.percentile(lat, 50)),
+               "worst_s": max(lat), "lengths": one_len}
     drv.free(ptr)
     return {"cubes": len(states), "cubes_per_s": len(states) / dt, "seconds": dt, "batch": batch,
             "nodes_per_cube": nodes / len(states), "table_build_s": build_s, "lengths": lengths,
+            "one_per_call": one,
             "note": f"reference kernels.cu (unmodified, nvcc sm_100) driven with its host loop, {batch} cubes per "
-                    "solve call, wall clock including its per-bound host round trips"}
+                    "solve call (and one per call for the first cubes), wall clock including its per-bound host "
+                    "round trips"}
 
 
 # ---------------------------------------------------------------------------------------------
@@ -512,12 +526,16 @@ def main_arm(args, world: int, rank: int, local: int) -> None:
 
     ref_gpu = None
     if args.ref_gpu and args.plain:
-        ref_gpu = reference_gpu_run(args.kind, args.format, plain_states, args.ref_batch, local)
+        ref_gpu = reference_gpu_run(args.kind, args.format, plain_states, args.ref_batch, local, args.ref_one)
         if "lengths" in ref_gpu:
             ref_gpu["lengths_equal_to_plain"] = ref_gpu.pop("lengths") == plain_len
             ref_gpu["ours_over_reference"] = {"batched": value / ref_gpu["cubes_per_s"],
                                               "e2e": e2e / ref_gpu["cubes_per_s"],
                                               "plain": plain["cubes_per_s"] / ref_gpu["cubes_per_s"]}
+            one = ref_gpu.get("one_per_call")
+            if one:
+                one["lengths_equal_to_plain"] = one.pop("lengths") == plain_len[: one["cubes"]]
+                ref_gpu["ours_over_reference"]["plain_over_one_per_call"] = plain["cubes_per_s"] / one["cubes_per_s"]
 
     # the same batch on d4 (second resident table) and with the flip-count rule
     mix = {config_table(args): {"cubes_per_s": value, "probes_per_s": roofline["probes_per_s"],
@@ -599,6 +617,8 @@ def main() -> None:
     ap.add_argument("--plain", type=int, default=1000, help="cubes solved one per call (0: skip)")
     ap.add_argument("--ref-gpu", type=int, default=1, help="1: time the reference's kernels.cu on the plain cubes")
     ap.add_argument("--ref-batch", type=int, default=100, help="reference kernels: cubes per solve call (its default)")
+    ap.add_argument("--ref-one", type=int, default=100,
+                    help="reference kernels: also solve this many plain cubes one per call (0: skip)")
     ap.add_argument("--second", default="d4", help="second resident table for the d4 leg and serving ('' for none)")
     ap.add_argument("--serve-s", type=float, default=8.0, help="seconds of arrivals per served rate (0: skip)")
     ap.add_argument("--serve-rates", default="10,50,100,200")
