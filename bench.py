@@ -307,6 +307,56 @@ def reference_gpu_run(kind: str, fmt: str, states, batch: int, device: int, one_
                     "round trips"}
 
 
+def presets_run(device: int, n_batch: int, n_plain: int) -> dict:
+    """Every preset end to end: GPU build written to a file, the file loaded back (warm page cache:
+    the double-buffered pinned copy), then n_batch uniform cubes (seed 2) in one batched solve
+    (device time) and n_plain of them one per call; lengths compared across the presets."""
+
+    import shutil
+    import tempfile
+
+    from cuda_cube_solver import kinds, native, workloads
+    from cuda_cube_solver.device import state_words
+
+    cubes = workloads.uniform_cubes(n_batch, seed=2)
+    words = state_words(cubes)
+    rows, ref_len = [], None
+    tmp = Path(tempfile.mkdtemp(prefix="ccs_presets_"))
+    try:
+        for p in kinds.PRESETS:
+            path = tmp / p.file
+            h = native.Handle(device)
+            try:
+                t0 = time.perf_counter()
+                counts, gpu_s = h.build_table(p.kind, p.format, path, keep_resident=False)
+                build_wall = time.perf_counter() - t0
+                t0 = time.perf_counter()
+                h.load_table(p.kind, p.format, path)
+                load_s = time.perf_counter() - t0
+                res = h.solve(words, native.solve_opts(timeout_s=900))
+                ms, probes, _ = h.last_solve_stats()
+                lengths = [r.length for r in res]
+                lat = []
+                for i in range(n_plain):
+                    t1 = time.perf_counter()
+                    h.solve(words[i:i + 1], native.solve_opts(timeout_s=120))
+                    lat.append(time.perf_counter() - t1)
+            finally:
+                h.close()
+                path.unlink(missing_ok=True)
+            ref_len = ref_len or lengths
+            rows.append({"preset": p.name, "table_gb": p.table_bytes / 1e9, "build_gpu_s": gpu_s,
+                         "build_and_write_s": build_wall, "load_s": load_s, "load_gb_s": p.table_bytes / 1e9 / load_s,
+                         "batched_cubes_per_s": n_batch / (ms / 1e3), "probes_per_s": probes / (ms / 1e3),
+                         "probes_per_cube": probes / n_batch,
+                         "plain_cubes_per_s": len(lat) / sum(lat) if lat else None,
+                         "plain_p50_s": float(np.percentile(lat, 50)) if lat else None,
+                         "lengths_equal_to_first": lengths == ref_len})
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return {"batch": n_batch, "plain": n_plain, "cubes": "uniform random cubes (seed 2)", "presets": rows}
+
+
 # ---------------------------------------------------------------------------------------------
 # arms
 
@@ -609,6 +659,10 @@ def main() -> None:
     ap.add_argument("--format", default="block", choices=["block", "b3"])
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference", "reference-gpu"])
+    ap.add_argument("--presets", action="store_true",
+                    help="instead of the bench: every preset built, loaded and solved (one JSON line)")
+    ap.add_argument("--preset-cubes", type=int, default=512)
+    ap.add_argument("--preset-plain", type=int, default=20)
     ap.add_argument("--variant", type=int, default=0, help="search kernel variant (ccs_solve_opts.variant)")
     ap.add_argument("--no-tune", dest="tune", action="store_false", help="skip the autotuner (library defaults)")
     ap.add_argument("--tune-budget", type=float, default=60.0, help="seconds of autotuning at most")
@@ -634,6 +688,10 @@ def main() -> None:
         args.second = ""  # (d4 beside d4t is the configuration's pair)
 
     world, rank, local = dist_setup()
+    if args.presets:
+        if rank == 0:
+            print(json.dumps({"mode": "presets", **presets_run(local, args.preset_cubes, args.preset_plain)}))
+        return
     if args.impl == "reference":
         reference_arm(args, world, rank, local)
         return
