@@ -193,6 +193,17 @@ extern "C" int ccs_solve_tables(ccs_handle* h, const uint32_t* states, const uin
     SearchParams P;
     fill_params(h, opts, &P);
     P.n_slots = (uint32_t)n;
+    if (n < 64) {
+        // Few cubes per call (the plain drop-in's shape) have their own defaults: a push or pop
+        // runs as soon as one lane waits for it, a probe pass repeats while 8 lanes probe, and
+        // deeper prefixes start 200x sooner while at most 4 cubes are in flight.  Measured on
+        // B200 (d4t, 256 x 2 with lookahead, 60 uniform cubes one per call): 55.0 cubes/s with the
+        // batch defaults (8 / 16 / 50); 58.0 with the first, 60.2 with the first two, 61.4 with
+        // the first and the third; a lone superflip 2.6 s either way.
+        if (!(opts && opts->move_min > 0)) P.move_min = 1u;
+        if (!(opts && opts->probe_min > 0)) P.probe_min = 8u;
+        if (!(opts && opts->few_divisor > 0)) P.few_divisor = 200u;
+    }
     cudaStream_t st = h->stream;
     CCS_CUDA_TRY(cudaMemcpyAsync(h->d_slots, host.data(), sizeof(Slot) * n, cudaMemcpyHostToDevice, st));
     CCS_CUDA_TRY(cudaMemsetAsync(h->d_ring, 0xFF, sizeof(unsigned long long) * (h->ring_cap + h->slot_cap), st));

@@ -167,10 +167,12 @@ typedef struct ccs_solve_opts {
                               /*   8 = lookahead 256 x 3 (4-5: loop-control forms)              */
     double shallow_at0;       /* an iteration of < this many nodes makes the next one use a    */
     double shallow_at1;       /*   prefix one move shorter (0: 1e5 / 1.5e6, < 0: off)          */
-    int move_min;             /* lanes waiting before a frame-update pass runs (0: 8)          */
+    int move_min;             /* lanes waiting before a frame-update pass runs (0: 8; 1 in a   */
+                              /*   ccs_solve of fewer than 64 cubes)                            */
     int move_age;             /* warp iterations a lane may wait for it (0: 4)                 */
     int probe_min;            /* a warp keeps probing (pruned children -> next sibling) while  */
-                              /*   at least this many lanes have a probe (0: default, > 32: off) */
+                              /*   at least this many lanes have a probe (0: 16, or 8 in a      */
+                              /*   ccs_solve of fewer than 64 cubes; > 32: off)                 */
     int steal;                /* work stealing: lanes donate unexplored subtrees to idle lanes  */
                               /*   (phase-ordered variants; 0 or 1: on, asked for by any idle   */
                               /*   lane; 2: on, asked for by whole idle warps; < 0: off).  The  */
@@ -181,7 +183,8 @@ typedef struct ccs_solve_opts {
                               /*   iterations, a power of two (0: 64)                           */
     int steal_target;         /* donors stop once this many subtrees wait (0: 512)              */
     int few_divisor;          /* while at most 4 cubes are in flight, deeper_at0/1 are divided */
-                              /*   by this (0: 50; 1: never, the reference's plain thresholds)  */
+                              /*   by this (0: 50, or 200 in a ccs_solve of fewer than 64       */
+                              /*   cubes; 1: never, the reference's plain thresholds)           */
     double steal_min_nodes;   /* subtrees of a cube are donated only once its previous          */
                               /*   iteration reached this many nodes (0: 1e7; < 0: always)      */
     int rotate;               /* a live entry at the work ring's head moves to the tail once   */
