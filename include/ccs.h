@@ -253,8 +253,8 @@ int ccs_probe_bench(ccs_handle* h, int n_states, int rounds, double* probes_per_
  * 1,048,575; each takes 456 bytes of device memory (cube slot and ring positions). */
 int ccs_server_start(ccs_handle* h, int slots, const ccs_solve_opts* opts);
 
-/* ccs_server_start with admission by device memory (the serving loop of north_star; the reference
- * has fixed --batch chunks only, __main__.py:129-133): the server holds a fixed footprint --
+/* ccs_server_start with admission by device memory (continuous batching; the reference has fixed
+ * --batch chunks only, __main__.py:129-133): the server holds a fixed footprint --
  * resident tables, constants, prefix lists, queue state, work-stealing cells and the persistent
  * launch's per-lane search stacks -- plus 456 bytes per cube in flight (its slot, ring positions
  * and admission entry); a cube is admitted only while the total stays within budget_bytes.

@@ -94,13 +94,13 @@ def main(ref: Path) -> None:
     (HERE / "host_model.json").write_text(json.dumps(host, separators=(",", ":")) + "\n")
 
     # Depth counts of the preset kinds (research/subgroups names, kinds.py:98).
-    survey = {"304": "g2-49", "s4": "g1-49", "d4f": "g1-43", "a4t": "g1-31", "d4t": "g1-27", "d4": "g1-26", "a4": "g1-30"}
+    subgroup = {"304": "g2-49", "s4": "g1-49", "d4f": "g1-43", "a4t": "g1-31", "d4t": "g1-27", "d4": "g1-26", "a4": "g1-30"}
     rows = {}
     for line in (ref / "research/subgroups/results.jsonl").read_text().splitlines():
         r = json.loads(line)
         rows[r["kind"]] = r
-    counts = {name: {"survey_name": sname, "entries": rows[sname]["entries"], "depth_counts": rows[sname]["depth_counts"],
-                     "block_exact": rows[sname].get("block_exact")} for name, sname in survey.items()}
+    counts = {name: {"subgroup_name": sname, "entries": rows[sname]["entries"], "depth_counts": rows[sname]["depth_counts"],
+                     "block_exact": rows[sname].get("block_exact")} for name, sname in subgroup.items()}
     (HERE / "depth_counts.json").write_text(json.dumps(counts, indent=1) + "\n")
 
     def solved_file(path):
