@@ -146,3 +146,52 @@ def test_gpusolver_refuses_unbuilt_reference_keywords():
                       ({"extra_kind": "s4"}, "extra_kind")):
         with pytest.raises(ValueError, match=match):
             GpuSolver(**kw)
+
+
+class _TableHandle:
+    """Stand-in for native.Handle that records the table calls (no device)."""
+
+    def __init__(self):
+        self.calls = []
+
+    def build_table_files(self, kind, block_path=None, b3_path=None, mod3_path=None, log=None):
+        self.calls.append(("build", kind, block_path, b3_path, mod3_path))
+        for p in (block_path, b3_path, mod3_path):
+            if p is not None:
+                p.write_bytes(b"")
+        return [1, 2, 18], 0.5
+
+    def encode_b3_file(self, kind, mod3_path, block_path, b3_path):
+        self.calls.append(("b3", kind, mod3_path, block_path, b3_path))
+        b3_path.write_bytes(b"\0" * 32)
+
+    def save_table(self, path, table=0):
+        self.calls.append(("save", path, table))
+
+    def table_histogram(self, table=0, n_bins=32):
+        self.calls.append(("hist", table, n_bins))
+        return [0] * n_bins
+
+
+def test_table_entry_points_use_the_reference_file_names(tmp_path, monkeypatch):
+    """table.build writes prune-ud-<kind>.bin (mod 3) and -blk.bin from one BFS plus the .json meta
+    (table.py:140-167); build_b3_table reads those two and writes -b3.bin (table.py:52-63);
+    save_device and histogram pass the table id through."""
+
+    from cuda_cube_solver import native, table
+
+    monkeypatch.setattr(native, "kind_info", lambda kind: (1, 9930 * 10))
+    h = _TableHandle()
+    mod3 = table.build(tmp_path, "d4t", log=None, handle=h)
+    assert mod3 == tmp_path / "prune-ud-d4t.bin"
+    assert h.calls[0] == ("build", "d4t", tmp_path / "prune-ud-d4t-blk.bin", None, mod3)
+    meta = json.loads(mod3.with_suffix(".json").read_text())
+    assert meta["depth_counts"] == [1, 2, 18] and meta["entries"] == 99300 and meta["classes"] == 9930
+    assert meta["encoding"] == "2-bit distance mod 3, 16 entries per little-endian uint32"
+    b3 = table.build_b3_table(tmp_path, "d4t", handle=h, log=lambda *_: None)
+    assert b3 == tmp_path / "prune-ud-d4t-b3.bin"
+    assert h.calls[1] == ("b3", "d4t", mod3, tmp_path / "prune-ud-d4t-blk.bin", b3)
+    table.save_device(h, tmp_path / "x.bin", table=1)
+    assert h.calls[2] == ("save", tmp_path / "x.bin", 1)
+    assert table.histogram(h, table=1, n_bins=24) == [0] * 24
+    assert h.calls[3] == ("hist", 1, 24)
