@@ -3,6 +3,7 @@ constants and errors behave like the reference's (no GPU work here)."""
 
 from __future__ import annotations
 
+import ctypes
 import re
 
 import numpy as np
@@ -59,3 +60,30 @@ def test_custom_group_kind_registration():
 def test_noalloc_limit_matches_header():
     text = (ROOT / "include" / "ccs.h").read_text()
     assert f"#define CCS_NOALLOC_MAX_CUBES {native.NOALLOC_MAX_CUBES}" in text
+
+
+def _header_fields(struct: str) -> list[tuple[str, str]]:
+    text = (ROOT / "include" / "ccs.h").read_text()
+    body = re.search(r"typedef struct " + struct + r" \{(.*?)\} " + struct + ";", text, re.S).group(1)
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    return re.findall(r"^\s*(int|double|int32_t|uint32_t|uint64_t|uint8_t)\s+(\w+)(?:\[\d+\])?;", body, re.M)
+
+
+def test_ctypes_structs_follow_the_header():
+    """The Python bindings' structures have the header's fields in the header's order and types
+    (the layout every FFI binding of ccs.h depends on)."""
+
+    ct = {"int": ctypes.c_int, "double": ctypes.c_double, "int32_t": ctypes.c_int32, "uint32_t": ctypes.c_uint32,
+          "uint64_t": ctypes.c_uint64}
+    for struct, cls in (("ccs_solve_opts", native.SolveOpts), ("ccs_result", native.Result),
+                        ("ccs_bfs_pass", native.BfsPass)):
+        header = _header_fields(struct)
+        fields = cls._fields_
+        assert [n for _, n in header] == [n for n, _ in fields], struct
+        for (ty, name), (_, cty) in zip(header, fields):
+            if ty == "uint8_t":  # arrays of bytes
+                assert issubclass(cty, ctypes.Array) and cty._type_ is ctypes.c_uint8, name
+            elif issubclass(cty, ctypes.Array):
+                assert cty._type_ is ct[ty], name
+            else:
+                assert cty is ct[ty], name
