@@ -212,9 +212,21 @@ extern "C" int ccs_last_build_passes(ccs_handle* h, ccs_bfs_pass* out, int max_o
 // One BFS of `kind`, then the files of paths[CCS_FMT_BLOCK / _B3 / _MOD3] (NULL: not written) and,
 // with keep_resident, the table of keep_format kept on the device (1: as the table, 2: as the
 // second table).
+// Puts a handle back on its resident table's kind when a build that did not replace that table
+// leaves (on success and on every error path alike).
+struct KindRestore {
+    ccs_handle* h;
+    std::string kind;
+    bool active = true;
+    ~KindRestore() {
+        if (active && h->d_table && !kind.empty() && h->kind_name != kind) set_kind(h, kind.c_str());
+    }
+};
+
 static int build_impl(ccs_handle* h, const char* kind, const char* const paths[3], int keep_format, int keep_resident,
                       uint64_t* depth_counts, int max_depths, int* n_depths, double* seconds, ccs_log_fn log) {
     const std::string first_kind = h->kind_ready ? h->kind_name : std::string();  // restored when a table stays
+    KindRestore restore{h, first_kind};
     CCS_TRY(set_kind(h, kind));
     CCS_CUDA_TRY(cudaSetDevice(h->device));
     const KindDesc k = h->kind;
@@ -366,14 +378,13 @@ static int build_impl(ccs_handle* h, const char* kind, const char* const paths[3
             h->d_table = d_out;
             h->table_bytes = kept_bytes;
             h->format = keep_format;
+            restore.active = false;  // the new table is of the new kind
         } else {
             std::string second = h->kind_name;
             rc = set_kind(h, first_kind.c_str());  // the constants stay those of the first table's kind
             if (rc == CCS_OK) rc = attach_second(h, second.c_str(), keep_format, d_out, kept_bytes);
             if (rc != CCS_OK) cudaFree(d_out);
         }
-    } else if (h->d_table && !first_kind.empty()) {
-        rc = set_kind(h, first_kind.c_str());  // a resident table keeps its kind's constants
     }
     return rc;
 }

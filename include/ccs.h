@@ -83,7 +83,8 @@ int ccs_load_table(ccs_handle* h, const char* kind, int format, const char* path
  * BFS, histogram self-check, encode in `format`.  If out_path is not NULL the solving file is
  * written there (through "<out_path>.tmp" and a rename).  If keep_resident, the solving table
  * stays loaded in the handle as if ccs_load_table had been called (keep_resident = 2: it becomes
- * the second table, see ccs_attach_table).  depth_counts receives up to
+ * the second table, see ccs_attach_table; with keep_resident = 0 a table already loaded keeps
+ * its kind, on success and on failure).  depth_counts receives up to
  * max_depths per-depth entry counts, n_depths their number; seconds the build time (GPU work,
  * without the file write).  log may be NULL. */
 int ccs_build_table(ccs_handle* h, const char* kind, int format, const char* out_path, int keep_resident,
@@ -91,8 +92,8 @@ int ccs_build_table(ccs_handle* h, const char* kind, int format, const char* out
 
 /* One BFS, several files (table.build, table.py:140-167, which writes the mod-3 and block files
  * of one generate): each non-NULL path is written from the same exact-depth array, through
- * "<path>.tmp" and a rename.  The handle's resident tables are left as they are; its kind becomes
- * `kind` (as after ccs_set_kind).  Counts, seconds and log as for ccs_build_table. */
+ * "<path>.tmp" and a rename.  The handle's resident tables are left as they are, and so is the
+ * kind they were loaded with.  Counts, seconds and log as for ccs_build_table. */
 int ccs_build_table_files(ccs_handle* h, const char* kind, const char* block_path, const char* b3_path,
                           const char* mod3_path, uint64_t* depth_counts, int max_depths, int* n_depths,
                           double* seconds, ccs_log_fn log);

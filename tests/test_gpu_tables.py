@@ -235,3 +235,22 @@ def test_reference_table_files_and_helpers(tmp_path, depth_golden):
             table.write_b3(short, blk, "304", tmp_path / "x-b3.bin", handle=h)
     finally:
         h.close()
+
+
+def test_building_another_kind_leaves_the_resident_table_usable(tmp_path):
+    """A build that keeps nothing (ccs_build_table with keep_resident 0, ccs_build_table_files)
+    leaves the loaded table answering with its own kind's constants."""
+
+    h = native.Handle()
+    try:
+        h.build_table("304", "block", None, keep_resident=True)
+        rng = np.random.default_rng(11)
+        states = [apply_moves(CubieState(), [MOVES_HTM[int(m)] for m in rng.integers(0, 18, 14)]) for _ in range(64)]
+        words = state_words(states)
+        before = h.lower_bound(words).tolist()
+        h.build_table("s4", "b3", None, keep_resident=False)
+        assert h.lower_bound(words).tolist() == before
+        h.build_table_files("s4", b3_path=tmp_path / "prune-ud-s4-b3.bin")
+        assert h.lower_bound(words).tolist() == before
+    finally:
+        h.close()
