@@ -16,7 +16,9 @@ Knobs (``native.SolveOpts``):
 * ``probe_min``: a warp keeps probing while at least this many lanes have a probe.
 
 Coordinate descent from the library defaults: each knob in turn takes the value with the best
-device time on the sample (the same cubes every time), within a time budget.  Results are cached
+device time on the sample (the same cubes every time), within a time budget; a value replaces the
+incumbent only when it is at least ``MIN_GAIN`` faster, so run-to-run noise on the sample does not
+move the settings away from the measured defaults.  Results are cached
 in a JSON file keyed by GPU name, table and batch-size bucket, and ``GpuSolver`` picks them up.
 """
 
@@ -41,6 +43,7 @@ SPACE = {
     "probe_min": [12, 16, 20, 24],
 }
 DEFAULT = {"variant": 3, "base_plen": 4, "move": (8, 4), "steal_depth": 2, "spread": 4096, "probe_min": 16}
+MIN_GAIN = 0.02  # a setting must cut the sample's device time by 2% to replace the incumbent
 
 
 def opts_of(cfg: dict, timeout_s: float = 600.0) -> native.SolveOpts:
@@ -88,7 +91,7 @@ def tune(handle: native.Handle, states, table: str, rounds: int = 2, log=None, b
                 trials.append((cfg, t))
                 if log:
                     log(f"{knob}={v}: {len(states) / t:8.1f} cubes/s")
-                if t < best_t:
+                if t < best_t * (1.0 - MIN_GAIN):
                     best, best_t = cfg, t
     return {"config": best, "cubes_per_s": len(states) / best_t, "trials": len(trials),
             "default_cubes_per_s": len(states) / trials[0][1], "complete": not out_of_time,

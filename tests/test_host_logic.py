@@ -41,6 +41,19 @@ def test_autotune_finds_the_best_settings():
     assert result["complete"]
 
 
+def test_autotune_ignores_gains_within_noise():
+    """A setting 1% faster than the incumbent does not replace it (the descent needs MIN_GAIN)."""
+
+    class Flat(FakeHandle):
+        def solve(self, words, opts):
+            self.calls.append(opts)
+            self._ms = 100.0 if opts.base_plen != 5 else 99.0
+            return []
+
+    result = autotune.tune(Flat(), workloads.uniform_cubes(4, seed=9), "d4t", rounds=1)
+    assert result["config"] == autotune.DEFAULT
+
+
 def test_autotune_stops_at_its_budget():
     h = FakeHandle()
     result = autotune.tune(h, workloads.uniform_cubes(4, seed=9), "d4t", rounds=2, budget_s=1e-9)
