@@ -481,6 +481,11 @@ def main_arm(args, world: int, rank: int, local: int) -> None:
 
     peaks = measured_peaks()
     config = workload_config(args, world)
+    if world > 1:
+        # the untimed legs (plain, the reference's kernels, the served stream, the d4 pair, the
+        # gather ceiling, the CPU baselines) are one-GPU measurements run by rank 0 while every
+        # other rank waits: at N > 1 the line carries the batched step alone
+        args.plain, args.ref_gpu, args.serve_s, args.second, args.no_ceiling, args.no_cpu = 0, 0, 0.0, "", True, True
 
     # ---- set-up (untimed): the table built on this GPU and kept resident; the workload ----
     t = time.perf_counter()
@@ -550,10 +555,12 @@ def main_arm(args, world: int, rank: int, local: int) -> None:
 
     # ---- after the timed region (untimed) ----
     words = state_words(cubes)
-    h.solve(state_words(workloads.uniform_cubes(1024, seed=args.seed)), opts)
-    ms, pr, _ = h.last_solve_stats()
-    uniform = {"cubes": 1024, "workload": f"uniform random cubes (seed {args.seed}) alone",
-               "cubes_per_s": 1024 / (ms / 1e3), "probes_per_s": pr / (ms / 1e3)}
+    uniform = None
+    if world == 1:
+        h.solve(state_words(workloads.uniform_cubes(1024, seed=args.seed)), opts)
+        ms, pr, _ = h.last_solve_stats()
+        uniform = {"cubes": 1024, "workload": f"uniform random cubes (seed {args.seed}) alone",
+                   "cubes_per_s": 1024 / (ms / 1e3), "probes_per_s": pr / (ms / 1e3)}
 
     plain = None
     plain_len = None
