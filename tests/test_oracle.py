@@ -113,3 +113,35 @@ def test_oracle_ida_star_with_trivial_bounds(oracle):
     for s, L, mv in zip(states, lengths, moves):
         assert L == dist[s]
         assert apply_moves(s, [MOVES_HTM[m] for m in mv[:L]]) == CubieState()
+
+
+def test_base3_from_the_mod3_and_block_tables(oracle):
+    """The reference's base-3 file is a function of its mod-3 and 2-bit block tables
+    (build_b3_table, table.py:52-79): recovering each entry's value from the pair (the block offset
+    below 3, else the smallest value >= minimum + 3 with the mod-3 residue) and encoding it gives
+    the same bytes as encoding from the exact depths; the mod-3 words hold depth mod 3, sixteen
+    two-bit entries per little-endian uint32, 3 past the end."""
+
+    rng = np.random.default_rng(21)
+    n = 155 * 40 + 17
+    base = np.repeat(rng.integers(4, 14, -(-n // 124)), 124)[:n]
+    depth = (base + rng.choice([0, 0, 1, 1, 2, 3, 4, 5, 6, 9], n)).astype(np.uint8)
+    blk = oracle.encode_block(depth)
+    direct = oracle.encode_b3(depth, blk)
+
+    padded = np.full(-(-n // 16) * 16, 3, np.uint32)
+    padded[:n] = depth % 3
+    mod3 = (padded.reshape(-1, 16) << (2 * np.arange(16, dtype=np.uint32))).sum(axis=1).astype(np.uint32)
+    assert int((mod3[-1] >> (2 * (n % 16))) & 3) == 3  # past the end
+
+    x = np.arange(n)
+    words = blk.view(np.uint32).reshape(-1, 8)
+    sec, j = x // 124, x % 124
+    pos = 8 + 2 * j
+    m = (words[sec, 0] & 0xFF).astype(np.int64)
+    off = ((words[sec, pos // 32] >> (pos % 32).astype(np.uint32)) & 3).astype(np.int64)
+    r = ((mod3[x // 16] >> (2 * (x % 16)).astype(np.uint32)) & 3).astype(np.int64)
+    lo = m + 3
+    value = np.where(off < 3, m + off, lo + (r - lo) % 3)
+    assert np.all(value[depth <= m + 5] == depth[depth <= m + 5])
+    assert np.array_equal(oracle.encode_b3(value.astype(np.uint8), blk), direct)
