@@ -555,12 +555,17 @@ def main_arm(args, world: int, rank: int, local: int) -> None:
 
     # ---- after the timed region (untimed) ----
     words = state_words(cubes)
-    uniform = None
+    uniform = uniform_full = None
     if world == 1:
         h.solve(state_words(workloads.uniform_cubes(1024, seed=args.seed)), opts)
         ms, pr, _ = h.last_solve_stats()
         uniform = {"cubes": 1024, "workload": f"uniform random cubes (seed {args.seed}) alone",
                    "cubes_per_s": 1024 / (ms / 1e3), "probes_per_s": pr / (ms / 1e3)}
+        # the batch size of the timed steps, all of it uniform (the hard positions left out)
+        h.solve(state_words(workloads.uniform_cubes(args.batch, seed=args.seed)), opts)
+        ms, pr, _ = h.last_solve_stats()
+        uniform_full = {"cubes": args.batch, "workload": f"uniform random cubes (seed {args.seed}) alone",
+                        "cubes_per_s": args.batch / (ms / 1e3), "probes_per_s": pr / (ms / 1e3)}
 
     plain = None
     plain_len = None
@@ -579,7 +584,8 @@ def main_arm(args, world: int, rank: int, local: int) -> None:
                  "cubes_per_s": rate, "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
                  "worst_s": max(lat), "probes_per_s": pl_probes / pl_dev if pl_dev else None,
                  "batched_over_plain": value / rate, "e2e_batched_over_plain": e2e / rate,
-                 "uniform_batched_over_plain": uniform["cubes_per_s"] / rate}
+                 "uniform_batched_over_plain": uniform_full["cubes_per_s"] / rate,
+                 "uniform_1024_over_plain": uniform["cubes_per_s"] / rate}
 
     ref_gpu = None
     if args.ref_gpu and args.plain:
@@ -645,7 +651,7 @@ def main_arm(args, world: int, rank: int, local: int) -> None:
            "lengths": {"histogram": {str(k): lengths.count(k) for k in sorted(set(lengths))},
                        "hard_equal_to_known": hard_ok, "equal_across_steps": True},
            "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
-           "batched_mix": mix, "uniform_1024": uniform, "plain": plain, "reference_gpu": ref_gpu, "served": served,
+           "batched_mix": mix, "uniform_1024": uniform, f"uniform_{args.batch}": uniform_full, "plain": plain, "reference_gpu": ref_gpu, "served": served,
            "table_build": {"kind": args.kind, "format": args.format, "gpu_seconds": solver.build_seconds,
                            "wall_s": build_wall_s, "entries": entries, "entries_per_s": entries / solver.build_seconds,
                            "table_bytes": h.table_bytes(), "depth_counts": solver.build_counts,
